@@ -1,0 +1,150 @@
+/* oneline_cuda.h — C ABI of the B200 (sm_100a) parse-and-search engine.
+ *
+ * Drop-in boundary for the oneline GPU path (tomet-lang/oneline, crate
+ * oneline-gpu). Every entry point takes plain pointers and sizes; no C++ or
+ * torch types cross it. Each declaration names the reference interface it
+ * replaces (file:line within the reference project).
+ *
+ * Conventions
+ *   - Every call returns an ol_status; OL_OK is 0. ol_last_error(ctx) gives a
+ *     message for the last failure on that context. A failed call never leaves
+ *     the context unusable (crates/oneline-gpu/src/tests.rs:353-373, 571-591).
+ *   - Output arrays are caller-allocated with an explicit capacity; true totals
+ *     are always returned even when the output was truncated.
+ *   - Handles (ol_ctx, ol_doc, ol_tree, ol_patset) are owned by the caller and
+ *     freed with the matching *_free / *_destroy call. Calls on one context are
+ *     serialized internally; handles may be used from any thread.
+ *   - Input text is copied to device memory; the host pointer is not retained.
+ */
+#ifndef ONELINE_CUDA_H
+#define ONELINE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t ol_status;
+enum {
+    OL_OK = 0,
+    OL_ERR_INVALID_ARG = 1,     /* null handle, bad flag, capacity too small where required */
+    OL_ERR_INPUT_TOO_LARGE = 2, /* text longer than OL_MAX_GPU_INPUT_LEN (util.rs:8-17) */
+    OL_ERR_BAD_PATTERN = 3,     /* empty pattern, bad set size or length (search.rs:41-46, many.rs:159-173) */
+    OL_ERR_TOO_DEEP = 4,        /* strict tree build: a content line has depth >= 32 (tree.rs:218-223) */
+    OL_ERR_OOM = 5,             /* device allocation failed */
+    OL_ERR_ADMISSION = 6,       /* a budgeted store refused the document */
+    OL_ERR_TIMEOUT = 7,         /* a bounded device wait ran out */
+    OL_ERR_CUDA = 8,            /* any other CUDA runtime error */
+    OL_ERR_NOT_FOUND = 9        /* unknown document id in a store */
+};
+
+/* NodeKind codes (crates/oneline-core/src/lib.rs:39-51). */
+enum {
+    OL_KIND_BLANK = 0, OL_KIND_TEXT = 1, OL_KIND_HEADING = 2, OL_KIND_ELEMENT = 3,
+    OL_KIND_LIST = 4, OL_KIND_CONNECT = 5, OL_KIND_ORDERED_LIST = 6, OL_KIND_COMMENT = 7
+};
+
+#define OL_NONE 0xFFFFFFFFu                  /* crates/oneline-core/src/links.rs:6 */
+#define OL_MAX_GPU_INPUT_LEN 0xFFFFFFFCull   /* u32::MAX - 3, crates/oneline-gpu/src/util.rs:8 */
+#define OL_MAX_PATTERN_LEN 64u               /* crates/oneline-gpu/src/lib.rs:66 (drop-in search limit) */
+#define OL_MAX_PATTERNS 2048u                /* crates/oneline-gpu/src/many.rs:14 (drop-in set limit) */
+#define OL_MIN_SET_PATTERN_LEN 4u            /* crates/oneline-gpu/src/many.rs:17 */
+#define OL_MAX_SET_PATTERN_LEN 64u           /* crates/oneline-gpu/src/many.rs:18 */
+#define OL_MAX_TREE_DEPTH 32u                /* crates/oneline-gpu/src/tree.rs:12 */
+
+/* FlatNode, 16 bytes (crates/oneline-core/src/lib.rs:86-96). */
+typedef struct ol_flat_node {
+    uint32_t depth;
+    uint32_t kind;
+    uint32_t span_start;
+    uint32_t span_len;
+} ol_flat_node;
+
+/* ManyHit (crates/oneline-gpu/src/many.rs:77-82). */
+typedef struct ol_hit {
+    uint32_t pattern;
+    uint32_t offset;
+} ol_hit;
+
+typedef struct ol_ctx ol_ctx;
+typedef struct ol_doc ol_doc;
+typedef struct ol_tree ol_tree;
+typedef struct ol_patset ol_patset;
+
+/* ---- context: GpuParser::new / adapter_name (crates/oneline-gpu/src/parser.rs:94-142, 470-479) */
+ol_status ol_ctx_create(int32_t device, ol_ctx **out);
+void ol_ctx_destroy(ol_ctx *ctx);
+const char *ol_last_error(const ol_ctx *ctx);
+ol_status ol_ctx_device_name(ol_ctx *ctx, char *buf, size_t cap);
+/* Blocks until every operation enqueued on the context's stream is done. */
+ol_status ol_ctx_sync(ol_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order work. */
+void *ol_ctx_stream(ol_ctx *ctx);
+
+/* ---- resident documents: GpuParser::upload, GpuDocument::{line_count,text_len}
+ *      (crates/oneline-gpu/src/document.rs:16-90, 111-127) */
+ol_status ol_doc_upload(ol_ctx *ctx, const uint8_t *text, uint64_t len, ol_doc **out);
+/* Same, for text already in this device's memory (copied device-to-device). */
+ol_status ol_doc_upload_device(ol_ctx *ctx, const uint8_t *dev_text, uint64_t len, ol_doc **out);
+void ol_doc_free(ol_doc *doc);
+uint64_t ol_doc_line_count(const ol_doc *doc);
+uint64_t ol_doc_text_len(const ol_doc *doc);
+/* Deepest non-blank line (0 for an empty document). */
+uint64_t ol_doc_max_depth(const ol_doc *doc);
+/* Re-runs the scan + classify kernels over the resident text into the
+ * document's own buffers, enqueued on the context stream without waiting. */
+ol_status ol_doc_reparse_async(ol_ctx *ctx, ol_doc *doc);
+/* Downloads: line_offsets (scan.rs:138-146), kinds (u8 NodeKind per line) and
+ * 16-byte nodes (parse.rs:69-80). cap = entries the output can hold; it must be
+ * at least the line count. */
+ol_status ol_doc_read_offsets(ol_ctx *ctx, const ol_doc *doc, uint32_t *out, uint64_t cap);
+ol_status ol_doc_read_kinds(ol_ctx *ctx, const ol_doc *doc, uint8_t *out, uint64_t cap);
+ol_status ol_doc_read_nodes(ol_ctx *ctx, const ol_doc *doc, ol_flat_node *out, uint64_t cap);
+/* Device pointers of a resident document (valid until ol_doc_free). */
+ol_status ol_doc_device_views(const ol_doc *doc, const uint8_t **text, const uint32_t **offsets, const uint8_t **kinds,
+                              const uint8_t **depth8);
+
+/* ---- one-shot parse: GpuParser::parse_raw, scan_line_offsets, parse(input, offsets)
+ *      (crates/oneline-gpu/src/parse.rs:86-125, scan.rs:127-136). *line_count
+ *      always receives the true count; outputs are written when cap allows. */
+ol_status ol_parse_raw(ol_ctx *ctx, const uint8_t *text, uint64_t len, uint32_t *offsets, ol_flat_node *nodes,
+                       uint64_t cap, uint64_t *line_count);
+ol_status ol_scan_line_offsets(ol_ctx *ctx, const uint8_t *text, uint64_t len, uint32_t *offsets, uint64_t cap,
+                               uint64_t *line_count);
+ol_status ol_parse_with_offsets(ol_ctx *ctx, const uint8_t *text, uint64_t len, const uint32_t *offsets,
+                                uint64_t n_lines, ol_flat_node *nodes);
+
+/* ---- tree: GpuParser::build_tree / build_tree_reusing / download_links,
+ *      GpuTree::line_count (crates/oneline-gpu/src/tree.rs:34-67, 278-290) */
+#define OL_TREE_STRICT_DEPTH 1u  /* fail with OL_ERR_TOO_DEEP like the reference when depth >= 32 */
+ol_status ol_tree_build(ol_ctx *ctx, const ol_doc *doc, uint32_t flags, ol_tree **out);
+/* Reuses `previous`'s buffers when large enough; `previous` is consumed (freed
+ * or adopted) whatever the outcome. */
+ol_status ol_tree_build_reusing(ol_ctx *ctx, const ol_doc *doc, ol_tree *previous, uint32_t flags, ol_tree **out);
+/* Re-runs the tree kernels for `doc` into `tree` (same line count), no wait. */
+ol_status ol_tree_rebuild_async(ol_ctx *ctx, const ol_doc *doc, ol_tree *tree);
+void ol_tree_free(ol_tree *tree);
+uint64_t ol_tree_line_count(const ol_tree *tree);
+/* Any output may be NULL. cap must be >= the line count. */
+ol_status ol_tree_read(ol_ctx *ctx, const ol_tree *tree, uint32_t *parent, uint32_t *subtree_end, uint32_t *first_child,
+                       uint32_t *next_sibling, uint64_t cap);
+
+/* ---- substring search: GpuParser::search_document / search_raw
+ *      (crates/oneline-gpu/src/search.rs:84-140). Any pattern length >= 1 is
+ *      accepted here (the reference's 64-byte cap is applied by the drop-in
+ *      wrappers). out receives the first min(total, max_matches) offsets in
+ *      ascending order. */
+ol_status ol_search(ol_ctx *ctx, const ol_doc *doc, const uint8_t *pattern, uint32_t pat_len, uint32_t max_matches,
+                    uint32_t *total, uint32_t *out);
+ol_status ol_search_raw(ol_ctx *ctx, const uint8_t *text, uint64_t len, const uint8_t *pattern, uint32_t pat_len,
+                        uint32_t max_matches, uint32_t *total, uint32_t *out);
+/* Enqueues the search without waiting: *d_total and d_out are device pointers. */
+ol_status ol_search_async(ol_ctx *ctx, const ol_doc *doc, const uint8_t *pattern, uint32_t pat_len,
+                          uint32_t max_matches, uint32_t *d_total, uint32_t *d_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ONELINE_CUDA_H */

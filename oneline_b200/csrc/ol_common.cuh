@@ -1,0 +1,232 @@
+// Device-side building blocks shared by the oneline sm_100a kernels.
+//
+// * NodeKind codes and FlatNode layout (crates/oneline-core/src/lib.rs:39-96).
+// * Decoupled look-back primitives: every tile publishes a 64-bit word
+//   [status:2 | value:32] per value it carries, readers poll with bounded spins.
+// * Device status words: a kernel never traps or spins forever; a wait that runs
+//   past its limit sets OL_DEVERR_TIMEOUT and the kernel finishes with garbage
+//   that the host discards after reading the status.
+#pragma once
+#include <cstdint>
+
+namespace ol {
+
+constexpr uint32_t NONE = 0xFFFFFFFFu;
+
+enum Kind : uint8_t {
+    KIND_BLANK = 0,
+    KIND_TEXT = 1,
+    KIND_HEADING = 2,
+    KIND_ELEMENT = 3,
+    KIND_LIST = 4,
+    KIND_CONNECT = 5,
+    KIND_ORDERED = 6,
+    KIND_COMMENT = 7,
+};
+
+struct FlatNode {
+    uint32_t depth, kind, span_start, span_len;
+};
+
+// Device status bits (DocStats::error and friends).
+constexpr uint32_t OL_DEVERR_TIMEOUT = 1u << 0;   // a bounded wait ran out
+constexpr uint32_t OL_DEVERR_CAPACITY = 1u << 1;  // an output buffer was too small
+constexpr uint32_t OL_DEVERR_FIXUP = 1u << 2;     // fix-up list overflow (cannot happen by construction)
+constexpr uint32_t OL_DEVERR_DEEP = 1u << 3;      // a content line deeper than the fast tree path handles
+
+// Per-launch counters that live in device memory next to a document.
+struct DocStats {
+    uint32_t ticket;            // dynamic tile counter of the parse kernel
+    uint32_t line_count;        // lines in the document
+    uint32_t max_content_depth; // deepest non-blank line (saturates at 0xFFFFFFFF)
+    uint32_t fixup_count;       // lines classified by the fix-up kernel
+    uint32_t error;             // OL_DEVERR_* bits
+    uint32_t tree_ticket_fwd;   // dynamic tile counters of the tree kernels
+    uint32_t tree_ticket_bwd;
+    uint32_t search_ticket;
+    uint32_t pad[8];
+};
+
+// ---------------------------------------------------------- memory access --
+
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t *p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed_u64(uint64_t *p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Streaming 16-byte load (read once: do not keep in L1).
+__device__ __forceinline__ uint4 ld_stream16(const void *p) {
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// ------------------------------------------------------------ look-back ----
+
+constexpr uint64_t LB_AGGREGATE = 1ull << 32;
+constexpr uint64_t LB_PREFIX = 2ull << 32;
+constexpr uint64_t LB_STATUS_MASK = 3ull << 32;
+// A wait gives up after this long (ns) or this many polls, whichever first.
+constexpr uint64_t LB_WAIT_NS = 1000000000ull;  // 1 s
+constexpr uint32_t LB_WAIT_POLLS = 1u << 26;
+
+// Waits until word `p` has a non-zero status; returns it. On timeout (or when
+// another block already reported an error) sets OL_DEVERR_TIMEOUT in *err and
+// returns a PREFIX word with value 0 so that the caller stops walking.
+__device__ __forceinline__ uint64_t lb_wait(const uint64_t *p, uint32_t *err) {
+    uint64_t w = ld_relaxed_u64(p);
+    if (w & LB_STATUS_MASK) return w;
+    uint64_t t0 = globaltimer_ns();
+    uint32_t ns = 32;
+    for (uint32_t polls = 0;; polls++) {
+        w = ld_relaxed_u64(p);
+        if (w & LB_STATUS_MASK) return w;
+        if ((polls & 63) == 63) {
+            if (ld_relaxed_u32(err) != 0 || globaltimer_ns() - t0 > LB_WAIT_NS || polls > LB_WAIT_POLLS) {
+                atomicOr(err, OL_DEVERR_TIMEOUT);
+                return LB_PREFIX;
+            }
+        }
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
+    }
+}
+
+// Sum look-back over tiles 0..tile-1 done by one full warp (32-tile windows).
+// Returns the exclusive prefix of `tile`; all lanes get it.
+__device__ __forceinline__ uint32_t lb_sum_exclusive(const uint64_t *status, uint32_t tile, uint32_t *err) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t acc = 0;
+    int64_t end = (int64_t)tile;  // window is [end-32, end)
+    while (end > 0) {
+        int64_t idx = end - 32 + (int64_t)lane;
+        uint64_t w = idx >= 0 ? lb_wait(status + idx, err) : LB_PREFIX;  // before tile 0: prefix 0
+        uint32_t is_prefix = __ballot_sync(0xFFFFFFFFu, (w & LB_STATUS_MASK) == LB_PREFIX);
+        uint32_t v = (uint32_t)w;
+        if (is_prefix) {
+            int hi = 31 - __clz(is_prefix);  // nearest prefix in the window
+            uint32_t take = (int)lane >= hi ? v : 0;
+            for (int o = 16; o > 0; o >>= 1) take += __shfl_xor_sync(0xFFFFFFFFu, take, o);
+            return acc + take;
+        }
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        acc += v;
+        end -= 32;
+    }
+    return acc;
+}
+
+// Per-lane look-back for lanes that each carry an independent value chain
+// (one value per tile per lane at status + tile*stride + lane). `op` combines
+// an older tile's value into the running value; walking stops at the first
+// PREFIX word. Each lane walks alone, so lanes may mix statuses safely.
+template <class Op>
+__device__ __forceinline__ uint32_t lb_lane_exclusive(const uint64_t *status, uint32_t tile, uint32_t stride,
+                                                      uint32_t identity, uint32_t *err, Op op) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t acc = identity;
+    for (int64_t t = (int64_t)tile - 1; t >= 0; t--) {
+        uint64_t w = lb_wait(status + (uint64_t)t * stride + lane, err);
+        acc = op((uint32_t)w, acc);
+        if ((w & LB_STATUS_MASK) == LB_PREFIX) break;
+    }
+    return acc;
+}
+
+// ------------------------------------------------------------ byte SWAR ----
+
+// High bit of each byte of x set exactly where that byte is zero.
+__device__ __forceinline__ uint32_t zero_bytes(uint32_t x) {
+    uint32_t y = (x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu;
+    return ~(y | x | 0x7F7F7F7Fu);
+}
+
+// 4-bit mask (bit i = byte i) of bytes of w equal to c4's byte.
+__device__ __forceinline__ uint32_t eq_mask4(uint32_t w, uint32_t c4) {
+    uint32_t z = zero_bytes(w ^ c4);  // bits 7,15,23,31
+    // gather bits 7,15,23,31 into 0..3
+    return ((z >> 7) & 1u) | ((z >> 14) & 2u) | ((z >> 21) & 4u) | ((z >> 28) & 8u);
+}
+
+// 16-bit mask of the bytes of a 16-byte vector equal to byte c.
+__device__ __forceinline__ uint32_t eq_mask16(uint4 v, uint32_t c4) {
+    return eq_mask4(v.x, c4) | (eq_mask4(v.y, c4) << 4) | (eq_mask4(v.z, c4) << 8) | (eq_mask4(v.w, c4) << 12);
+}
+
+__device__ __forceinline__ bool is_blank(uint8_t b) { return b == ' ' || b == '\t'; }
+
+// classify_line (crates/oneline-simd/src/line.rs:57-81) on the first content
+// bytes c0, c1, c2; n = content length (bytes at index >= n do not exist).
+__device__ __forceinline__ uint8_t classify3(uint8_t c0, uint8_t c1, uint8_t c2, uint32_t n) {
+    switch (c0) {
+    case '=': return KIND_HEADING;
+    case ':': return KIND_CONNECT;
+    case '@': return KIND_ELEMENT;
+    case '/': return (n > 1 && c1 == '/') ? KIND_COMMENT : KIND_TEXT;
+    case '-':
+        if (n > 1 && is_blank(c1)) return KIND_LIST;
+        if (n > 2 && c1 == '.' && is_blank(c2)) return KIND_ORDERED;
+        return KIND_TEXT;
+    default: return KIND_TEXT;
+    }
+}
+
+// One line [s, e) where e is the position of its terminating '\n' or the text
+// end, read through `at(pos)`. Implements parse_line (line.rs:8-44):
+//   * the trailing run of '\r' before e is dropped (e itself is '\n' or end);
+//   * a line starting with '|' has a prefix made of the maximal run of '|' and
+//     blanks; its depth is the number of '|' in it, the content starts after it;
+//   * otherwise the depth is 0 and the content starts after leading blanks;
+//   * empty content gives Blank with the depth kept.
+template <class At>
+__device__ __forceinline__ FlatNode classify_line(uint32_t s, uint32_t e, At at) {
+    uint32_t eff = e;
+    while (eff > s && at(eff - 1) == '\r') eff--;
+    uint32_t c = s, depth = 0;
+    if (c < eff && at(c) == '|') {
+        while (c < eff) {
+            uint8_t b = at(c);
+            if (b == '|') depth++;
+            else if (!is_blank(b)) break;
+            c++;
+        }
+    } else {
+        while (c < eff && is_blank(at(c))) c++;
+    }
+    FlatNode nd;
+    nd.depth = depth;
+    nd.span_start = c;
+    if (c == eff) {
+        nd.kind = KIND_BLANK;
+        nd.span_len = 0;
+        return nd;
+    }
+    uint32_t n = eff - c;
+    uint8_t c0 = at(c);
+    uint8_t c1 = n > 1 ? at(c + 1) : 0;
+    uint8_t c2 = n > 2 ? at(c + 2) : 0;
+    nd.kind = classify3(c0, c1, c2, n);
+    nd.span_len = n;
+    return nd;
+}
+
+}  // namespace ol

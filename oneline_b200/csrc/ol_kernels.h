@@ -1,0 +1,88 @@
+// Kernel argument blocks and launch entry points shared between the kernels
+// (*.cu) and the host runtime (runtime.cu). Device pointers only.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace ol {
+
+struct FlatNode;
+struct DocStats;
+
+constexpr uint32_t kParseTile = 16384;  // text bytes per parse tile
+constexpr uint32_t kParseHalo = 256;    // bytes staged past a tile
+constexpr uint32_t kTreeTile = 4096;    // lines per tree tile (256 threads x 16)
+constexpr uint32_t kTreeLevels = 32;    // depth levels of the fast tree path
+
+struct ParseArgs {
+    const uint8_t *text;  // padded: n_tiles * kParseTile + kParseHalo readable bytes
+    uint64_t text_len;
+    uint32_t n_tiles;
+    uint64_t *tile_status;  // n_tiles words, zeroed before the launch
+    DocStats *stats;        // ticket/fixup_count/error zeroed before the launch
+    uint32_t *offsets;      // line_cap entries
+    uint8_t *kinds;
+    uint8_t *depth8;        // min(depth, 255)
+    FlatNode *nodes;        // optional (nullptr): full 16-byte nodes
+    uint32_t line_cap;
+    uint2 *fixup;           // (line index, start) of lines longer than the halo
+    uint32_t fixup_cap;
+};
+
+cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st);
+cudaError_t launch_classify_lines(const uint8_t *text, uint64_t N, const uint32_t *offsets, uint32_t L, FlatNode *nodes,
+                                  uint32_t *depth32, cudaStream_t st);
+
+struct TreeArgs {
+    const uint8_t *kinds;
+    const uint8_t *depth8;
+    uint32_t L;
+    uint32_t n_tiles;        // ceil(L / kTreeTile)
+    uint64_t *status_fwd;    // n_tiles * kTreeLevels words, zeroed
+    uint64_t *status_bwd;    // n_tiles * kTreeLevels words, zeroed
+    DocStats *stats;         // tree tickets zeroed
+    uint32_t *parent;
+    uint8_t *pdepth;         // depth of the parent, 0xFF for none
+    uint32_t *subtree_end;   // optional
+    uint32_t *first_child;
+    uint32_t *next_sibling;
+};
+
+cudaError_t launch_tree_fast(const TreeArgs &a, cudaStream_t st);
+
+// Any-depth path (content lines deeper than kTreeLevels-1).
+struct TreeDeepArgs {
+    const uint32_t *keys;    // depth of content lines, NONE for blank lines
+    uint32_t L;
+    uint32_t *levels[8];     // levels[0] = keys, levels[k] = min over 32 of levels[k-1]
+    uint32_t level_len[8];
+    uint32_t n_levels;
+    uint32_t *parent;
+    uint32_t *subtree_end;
+    uint32_t *first_child;
+    uint32_t *next_sibling;
+};
+
+cudaError_t launch_tree_deep(const TreeDeepArgs &a, cudaStream_t st);
+
+struct SearchArgs {
+    const uint8_t *text;     // padded like ParseArgs::text plus the pattern halo
+    uint64_t text_len;
+    const uint8_t *pattern;  // device copy
+    uint32_t pat_len;
+    uint32_t n_tiles;
+    uint64_t *tile_status;   // n_tiles words, zeroed
+    uint32_t *ticket;        // zeroed
+    uint32_t *total;         // written by the last tile
+    uint32_t *error;
+    uint32_t *out;           // ascending offsets, first max_out of them
+    uint32_t max_out;
+};
+
+constexpr uint32_t kSearchTile = 16384;
+constexpr uint32_t kSearchMaxStagedPattern = 4096;
+
+cudaError_t launch_search(const SearchArgs &a, cudaStream_t st);
+
+}  // namespace ol

@@ -1,0 +1,85 @@
+// Host-side state behind the C ABI handles.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "../../include/oneline_cuda.h"
+#include "ol_common.cuh"
+#include "ol_kernels.h"
+
+namespace ol {
+
+constexpr int kRingSlots = 4;
+constexpr uint64_t kRingBytes = 16ull << 20;  // 4 x 16 MiB pinned staging ring
+constexpr uint64_t kTextPad = kSearchMaxStagedPattern + kParseHalo + 64;
+
+// A device allocation from the stream-ordered pool, grown on demand.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t need, cudaStream_t st);
+    void release(cudaStream_t st);
+};
+
+// Small per-context device counters for searches and trees.
+struct CtxCounters {
+    uint32_t ticket;
+    uint32_t total;
+    uint32_t error;
+    uint32_t pad[13];
+};
+
+}  // namespace ol
+
+struct ol_ctx {
+    int device = 0;
+    int sm_count = 0;
+    char name[256] = {0};
+    cudaStream_t stream = nullptr;
+    std::recursive_mutex mu;
+    std::string last_error;
+    ol::DevBuf scratch_a;  // tile status words
+    ol::DevBuf scratch_b;  // second status array / uploaded offsets
+    ol::DevBuf scratch_c;  // nodes and other per-call outputs
+    ol::DevBuf search_out;
+    ol::DevBuf pattern_dev;
+    ol::CtxCounters *counters = nullptr;
+    ol::CtxCounters *host_counters = nullptr;  // pinned
+    uint8_t *ring[ol::kRingSlots] = {nullptr};
+    cudaEvent_t ring_done[ol::kRingSlots] = {nullptr};
+};
+
+struct ol_doc {
+    ol_ctx *ctx = nullptr;
+    uint64_t text_len = 0;
+    uint32_t line_count = 0;
+    uint32_t max_depth = 0;
+    uint32_t line_cap = 0;
+    ol::DevBuf text_buf, misc_buf, offsets_buf, kinds_buf, depth8_buf;
+    uint8_t *text = nullptr;
+    uint32_t *offsets = nullptr;
+    uint8_t *kinds = nullptr;
+    uint8_t *depth8 = nullptr;
+    ol::DocStats *stats = nullptr;
+    uint2 *fixup = nullptr;
+    ol::DocStats host_stats{};
+};
+
+struct ol_tree {
+    ol_ctx *ctx = nullptr;
+    uint32_t line_count = 0;
+    uint32_t capacity = 0;
+    bool deep = false;
+    ol::DevBuf parent_buf, pdepth_buf, end_buf, fc_buf, ns_buf;
+};
+
+namespace ol {
+ol_status ctx_fail(ol_ctx *ctx, ol_status code, const std::string &msg);
+ol_status ctx_cuda(ol_ctx *ctx, cudaError_t e, const char *what);
+uint32_t parse_tiles(uint64_t len);
+uint32_t round_lines(uint64_t n);
+ol_status new_text_doc(ol_ctx *ctx, const uint8_t *text, uint64_t len, ol_doc **out);
+}  // namespace ol

@@ -1,0 +1,309 @@
+"""GpuParser and friends: the public API of crates/oneline-gpu, over the C ABI.
+
+Method names, argument meaning and error behaviour follow the reference:
+
+* ``GpuParser.upload`` / ``GpuDocument``               document.rs:16-90, 111-127
+* ``GpuParser.parse_raw`` / ``parse`` / ``scan_line_offsets``  parse.rs:86-125, scan.rs:127-136
+* ``GpuParser.build_tree`` / ``build_tree_reusing`` / ``download_links`` / ``GpuTree``
+                                                        tree.rs:34-67, 278-290
+* ``GpuParser.search_document`` / ``search_raw`` / ``SearchResult``  search.rs:12-140
+* limits ``MAX_PATTERN_LEN``, ``MAX_TREE_DEPTH``, ``MAX_GPU_INPUT_LEN``  lib.rs:66, tree.rs:12, util.rs:8
+
+Errors are raised as ``OnelineError`` (the reference returns ``anyhow::Error``);
+a failed call leaves the parser usable. Every computation runs in the CUDA
+library; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import OnelineError, check
+from .core import NODE_DTYPE, NONE, FlatTree, TreeLinks
+
+MAX_PATTERN_LEN = 64
+MAX_TREE_DEPTH = 32
+MAX_GPU_INPUT_LEN = 0xFFFFFFFF - 3
+TREE_STRICT_DEPTH = 1
+
+
+def _as_bytes_view(data) -> tuple[int, int, object, bytes | np.ndarray]:
+    """(pointer, length, keepalive, source) for str / bytes / bytearray / uint8 arrays."""
+    if isinstance(data, str):
+        data = data.encode("utf-8")
+    if isinstance(data, np.ndarray):
+        a = np.ascontiguousarray(data, dtype=np.uint8).reshape(-1)
+        return a.ctypes.data, a.size, a, a
+    if isinstance(data, (bytes, bytearray, memoryview)):
+        b = bytes(data)
+        if not b:
+            return 0, 0, b, b
+        a = np.frombuffer(b, dtype=np.uint8)
+        return a.ctypes.data, a.size, a, b
+    raise TypeError(f"expected str, bytes or a uint8 array, got {type(data).__name__}")
+
+
+def _check_len(n: int) -> None:
+    if n > MAX_GPU_INPUT_LEN:
+        raise OnelineError(2, f"input is {n} bytes; the GPU path addresses at most {MAX_GPU_INPUT_LEN} bytes "
+                              "(32-bit offsets)")
+
+
+@dataclass
+class SearchResult:
+    """Substring search result (search.rs:12-21). ``offsets`` ascend; when
+    truncated by ``max_matches`` they are the lowest ``max_matches`` offsets."""
+
+    total_matches: int
+    offsets: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint32))
+
+    def __eq__(self, other) -> bool:
+        return (isinstance(other, SearchResult) and self.total_matches == other.total_matches
+                and np.array_equal(self.offsets, other.offsets))
+
+
+class GpuDocument:
+    """A document parsed once and kept in device memory (document.rs:16-127)."""
+
+    def __init__(self, parser: "GpuParser", handle: int, source):
+        self._parser = parser
+        self._h = handle
+        self._source = source
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def line_count(self) -> int:
+        return int(_lib.load().ol_doc_line_count(self._h))
+
+    def text_len(self) -> int:
+        return int(_lib.load().ol_doc_text_len(self._h))
+
+    def max_depth(self) -> int:
+        return int(_lib.load().ol_doc_max_depth(self._h))
+
+    def read_offsets(self) -> np.ndarray:
+        n = self.line_count()
+        out = np.zeros(max(n, 1), np.uint32)
+        check(_lib.load().ol_doc_read_offsets(self._parser._ctx, self._h, out.ctypes.data, out.size), self._parser._ctx)
+        return out[:n]
+
+    def read_kinds(self) -> np.ndarray:
+        n = self.line_count()
+        out = np.zeros(max(n, 1), np.uint8)
+        check(_lib.load().ol_doc_read_kinds(self._parser._ctx, self._h, out.ctypes.data, out.size), self._parser._ctx)
+        return out[:n]
+
+    def read_nodes(self) -> np.ndarray:
+        n = self.line_count()
+        out = np.zeros(max(n, 1), NODE_DTYPE)
+        check(_lib.load().ol_doc_read_nodes(self._parser._ctx, self._h, out.ctypes.data, out.size), self._parser._ctx)
+        return out[:n]
+
+    def free(self) -> None:
+        if self._h:
+            _lib.load().ol_doc_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class GpuTree:
+    """Tree links of a resident document (tree.rs:29-46)."""
+
+    def __init__(self, parser: "GpuParser", handle: int):
+        self._parser = parser
+        self._h = handle
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def line_count(self) -> int:
+        return int(_lib.load().ol_tree_line_count(self._h))
+
+    def _take(self) -> int:
+        h, self._h = self._h, None
+        return h
+
+    def free(self) -> None:
+        if self._h:
+            _lib.load().ol_tree_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class GpuParser:
+    """Parser and search engine on one CUDA device (parser.rs:8-142)."""
+
+    def __init__(self, device: int = 0):
+        L = _lib.load()
+        h = ctypes.c_void_p()
+        st = L.ol_ctx_create(device, ctypes.byref(h))
+        if st != 0:
+            raise OnelineError(st, f"cannot create a CUDA context on device {device}")
+        self._ctx = h.value
+
+    @classmethod
+    def new(cls, device: int = 0) -> "GpuParser":
+        return cls(device)
+
+    def close(self) -> None:
+        if getattr(self, "_ctx", None):
+            _lib.load().ol_ctx_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def ctx(self) -> int:
+        return self._ctx
+
+    def adapter_name(self) -> str:
+        buf = ctypes.create_string_buffer(256)
+        check(_lib.load().ol_ctx_device_name(self._ctx, buf, 256), self._ctx)
+        return buf.value.decode()
+
+    def is_software(self) -> bool:
+        return False
+
+    def timestamps_supported(self) -> bool:
+        return True
+
+    def sync(self) -> None:
+        check(_lib.load().ol_ctx_sync(self._ctx), self._ctx)
+
+    # ------------------------------------------------------------ documents
+
+    def upload(self, text) -> GpuDocument:
+        p, n, keep, src = _as_bytes_view(text)
+        _check_len(n)
+        h = ctypes.c_void_p()
+        check(_lib.load().ol_doc_upload(self._ctx, p, n, ctypes.byref(h)), self._ctx)
+        return GpuDocument(self, h.value, src)
+
+    def upload_device(self, dev_ptr: int, n: int) -> GpuDocument:
+        """Upload from this device's memory (e.g. a torch CUDA uint8 tensor's data_ptr)."""
+        _check_len(n)
+        h = ctypes.c_void_p()
+        check(_lib.load().ol_doc_upload_device(self._ctx, dev_ptr, n, ctypes.byref(h)), self._ctx)
+        return GpuDocument(self, h.value, None)
+
+    def parse_raw(self, text) -> FlatTree:
+        p, n, keep, src = _as_bytes_view(text)
+        _check_len(n)
+        L = _lib.load()
+        cnt = ctypes.c_uint64()
+        check(L.ol_parse_raw(self._ctx, p, n, None, None, 0, ctypes.byref(cnt)), self._ctx)
+        lines = cnt.value
+        offs = np.zeros(max(lines, 1), np.uint32)
+        nodes = np.zeros(max(lines, 1), NODE_DTYPE)
+        if lines:
+            check(L.ol_parse_raw(self._ctx, p, n, offs.ctypes.data, nodes.ctypes.data, lines, ctypes.byref(cnt)), self._ctx)
+        return FlatTree(src if isinstance(src, bytes) else bytes(src), nodes[:lines], offs[:lines])
+
+    def parse(self, text, line_offsets) -> FlatTree:
+        p, n, keep, src = _as_bytes_view(text)
+        _check_len(n)
+        offs = np.ascontiguousarray(line_offsets, np.uint32)
+        nodes = np.zeros(max(offs.size, 1), NODE_DTYPE)
+        if offs.size:
+            check(_lib.load().ol_parse_with_offsets(self._ctx, p, n, offs.ctypes.data, offs.size, nodes.ctypes.data),
+                  self._ctx)
+        return FlatTree(src if isinstance(src, bytes) else bytes(src), nodes[: offs.size], offs.copy())
+
+    def scan_line_offsets(self, text) -> np.ndarray:
+        p, n, keep, src = _as_bytes_view(text)
+        _check_len(n)
+        L = _lib.load()
+        cnt = ctypes.c_uint64()
+        check(L.ol_scan_line_offsets(self._ctx, p, n, None, 0, ctypes.byref(cnt)), self._ctx)
+        out = np.zeros(max(cnt.value, 1), np.uint32)
+        if cnt.value:
+            check(L.ol_scan_line_offsets(self._ctx, p, n, out.ctypes.data, out.size, ctypes.byref(cnt)), self._ctx)
+        return out[: cnt.value]
+
+    # ----------------------------------------------------------------- tree
+
+    def build_tree(self, doc: GpuDocument, *, strict_depth: bool = True) -> GpuTree:
+        """Tree links of `doc`. Like the reference, a content line nested 32 or more
+        levels deep is an error unless ``strict_depth=False`` (then any depth works)."""
+        return self.build_tree_reusing(doc, None, strict_depth=strict_depth)
+
+    def build_tree_reusing(self, doc: GpuDocument, previous: GpuTree | None, *, strict_depth: bool = True) -> GpuTree:
+        h = ctypes.c_void_p()
+        prev = previous._take() if previous is not None else None
+        flags = TREE_STRICT_DEPTH if strict_depth else 0
+        check(_lib.load().ol_tree_build_reusing(self._ctx, doc.handle, prev, flags, ctypes.byref(h)), self._ctx)
+        return GpuTree(self, h.value)
+
+    def _read_tree(self, tree: GpuTree, which: tuple[str, ...]) -> dict:
+        n = tree.line_count()
+        arrs = {k: np.zeros(max(n, 1), np.uint32) for k in which}
+        ptr = lambda k: arrs[k].ctypes.data if k in arrs else None  # noqa: E731
+        check(_lib.load().ol_tree_read(self._ctx, tree.handle, ptr("parent"), ptr("subtree_end"), ptr("first_child"),
+                                       ptr("next_sibling"), max(n, 1)), self._ctx)
+        return {k: v[:n] for k, v in arrs.items()}
+
+    def download_links(self, tree: GpuTree) -> TreeLinks:
+        a = self._read_tree(tree, ("parent", "subtree_end"))
+        return TreeLinks(a["parent"], a["subtree_end"])
+
+    def download_tree(self, tree: GpuTree) -> dict:
+        """parent, subtree_end, first_child and next_sibling of every line."""
+        return self._read_tree(tree, ("parent", "subtree_end", "first_child", "next_sibling"))
+
+    # --------------------------------------------------------------- search
+
+    @staticmethod
+    def _check_pattern(pattern: bytes, max_len: int | None) -> bytes:
+        pattern = pattern.encode() if isinstance(pattern, str) else bytes(pattern)
+        if not pattern or (max_len is not None and len(pattern) > max_len):
+            lim = max_len if max_len is not None else "any"
+            raise OnelineError(3, f"pattern must be 1..={lim} bytes, got {len(pattern)}")
+        return pattern
+
+    def search_document(self, doc: GpuDocument, pattern: bytes, max_matches: int, *,
+                        max_pattern_len: int | None = MAX_PATTERN_LEN) -> SearchResult:
+        """Every (overlapping) occurrence of `pattern` in a resident document.
+        The reference accepts 1..=64 bytes; pass ``max_pattern_len=None`` for any length."""
+        pattern = self._check_pattern(pattern, max_pattern_len)
+        if max_matches > 0xFFFFFFFF:
+            raise OnelineError(1, f"max_matches {max_matches} does not fit in u32")
+        out = np.zeros(max(max_matches, 1), np.uint32)
+        total = ctypes.c_uint32()
+        pa = np.frombuffer(pattern, np.uint8)
+        check(_lib.load().ol_search(self._ctx, doc.handle, pa.ctypes.data, len(pattern), max_matches,
+                                    ctypes.byref(total), out.ctypes.data), self._ctx)
+        k = min(total.value, max_matches)
+        return SearchResult(total.value, out[:k].copy())
+
+    def search_raw(self, text, pattern: bytes, max_matches: int, *,
+                   max_pattern_len: int | None = MAX_PATTERN_LEN) -> SearchResult:
+        p, n, keep, src = _as_bytes_view(text)
+        _check_len(n)
+        pattern = self._check_pattern(pattern, max_pattern_len)
+        out = np.zeros(max(max_matches, 1), np.uint32)
+        total = ctypes.c_uint32()
+        pa = np.frombuffer(pattern, np.uint8)
+        check(_lib.load().ol_search_raw(self._ctx, p, n, pa.ctypes.data, len(pattern), max_matches,
+                                        ctypes.byref(total), out.ctypes.data), self._ctx)
+        k = min(total.value, max_matches)
+        return SearchResult(total.value, out[:k].copy())
