@@ -143,6 +143,15 @@ ol_status ol_search_raw(ol_ctx *ctx, const uint8_t *text, uint64_t len, const ui
 /* Enqueues the search without waiting: *d_total and d_out are device pointers. */
 ol_status ol_search_async(ol_ctx *ctx, const ol_doc *doc, const uint8_t *pattern, uint32_t pat_len,
                           uint32_t max_matches, uint32_t *d_total, uint32_t *d_out);
+/* n patterns in one call (up to eight share each pass over the text); per
+ * pattern i: totals[i] and the first min(totals[i], max_matches[i]) offsets in
+ * outs[i], ascending. Extension of search_document for callers with several
+ * patterns (no single reference counterpart; semantics per pattern as above). */
+ol_status ol_search_multi(ol_ctx *ctx, const ol_doc *doc, const uint8_t *const *patterns, const uint32_t *lens,
+                          uint32_t n, const uint32_t *max_matches, uint32_t *totals, uint32_t *const *outs);
+/* Same, enqueued without waiting; d_totals (n entries) and d_outs[i] are device pointers. */
+ol_status ol_search_multi_async(ol_ctx *ctx, const ol_doc *doc, const uint8_t *const *patterns, const uint32_t *lens,
+                                uint32_t n, const uint32_t *max_matches, uint32_t *d_totals, uint32_t *const *d_outs);
 
 #ifdef __cplusplus
 }

@@ -58,6 +58,8 @@ SIGNATURES: dict[str, tuple] = {
     "ol_search": (_S, [_P, _P, _U8P, _U32, _U32, _U32P, _P]),
     "ol_search_raw": (_S, [_P, _U8P, _U64, _U8P, _U32, _U32, _U32P, _P]),
     "ol_search_async": (_S, [_P, _P, _U8P, _U32, _U32, _P, _P]),
+    "ol_search_multi": (_S, [_P, _P, _P, _P, _U32, _P, _P, _P]),
+    "ol_search_multi_async": (_S, [_P, _P, _P, _P, _U32, _P, _P, _P]),
 }
 
 _lib = None

@@ -112,14 +112,16 @@ __device__ __forceinline__ uint64_t lb_wait(const uint64_t *p, uint32_t *err) {
 }
 
 // Sum look-back over tiles 0..tile-1 done by one full warp (32-tile windows).
-// Returns the exclusive prefix of `tile`; all lanes get it.
-__device__ __forceinline__ uint32_t lb_sum_exclusive(const uint64_t *status, uint32_t tile, uint32_t *err) {
+// Tile t's word is status[t * stride]. Returns the exclusive prefix of `tile`;
+// all lanes get it.
+__device__ __forceinline__ uint32_t lb_sum_exclusive(const uint64_t *status, uint32_t tile, uint32_t *err,
+                                                     uint32_t stride = 1) {
     const uint32_t lane = threadIdx.x & 31;
     uint32_t acc = 0;
     int64_t end = (int64_t)tile;  // window is [end-32, end)
     while (end > 0) {
         int64_t idx = end - 32 + (int64_t)lane;
-        uint64_t w = idx >= 0 ? lb_wait(status + idx, err) : LB_PREFIX;  // before tile 0: prefix 0
+        uint64_t w = idx >= 0 ? lb_wait(status + idx * stride, err) : LB_PREFIX;  // before tile 0: prefix 0
         uint32_t is_prefix = __ballot_sync(0xFFFFFFFFu, (w & LB_STATUS_MASK) == LB_PREFIX);
         uint32_t v = (uint32_t)w;
         if (is_prefix) {

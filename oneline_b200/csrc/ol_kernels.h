@@ -24,7 +24,6 @@ struct ParseArgs {
     uint32_t *offsets;      // line_cap entries
     uint8_t *kinds;
     uint8_t *depth8;        // min(depth, 255)
-    FlatNode *nodes;        // optional (nullptr): full 16-byte nodes
     uint32_t line_cap;
     uint2 *fixup;           // (line index, start) of lines longer than the halo
     uint32_t fixup_cap;
@@ -66,22 +65,24 @@ struct TreeDeepArgs {
 
 cudaError_t launch_tree_deep(const TreeDeepArgs &a, cudaStream_t st);
 
-struct SearchArgs {
-    const uint8_t *text;     // padded like ParseArgs::text plus the pattern halo
-    uint64_t text_len;
-    const uint8_t *pattern;  // device copy
-    uint32_t pat_len;
-    uint32_t n_tiles;
-    uint64_t *tile_status;   // n_tiles words, zeroed
-    uint32_t *ticket;        // zeroed
-    uint32_t *total;         // written by the last tile
-    uint32_t *error;
-    uint32_t *out;           // ascending offsets, first max_out of them
-    uint32_t max_out;
-};
-
 constexpr uint32_t kSearchTile = 16384;
 constexpr uint32_t kSearchMaxStagedPattern = 4096;
+constexpr uint32_t kSearchMaxPatterns = 8;  // patterns per launch
+
+struct SearchArgs {
+    const uint8_t *text;     // padded: n_tiles * kSearchTile + kSearchMaxStagedPattern + 16 readable bytes
+    uint64_t text_len;
+    uint32_t n_tiles;
+    uint32_t np;                                // patterns in this launch (1..8)
+    uint32_t halo;                              // round_up(longest - 1, 16); > 4096 only when np == 1
+    const uint8_t *pat[kSearchMaxPatterns];     // device copies
+    uint32_t pat_len[kSearchMaxPatterns];
+    uint32_t *out[kSearchMaxPatterns];          // ascending offsets, first max_out[p] of them
+    uint32_t max_out[kSearchMaxPatterns];
+    uint64_t *tile_status;   // n_tiles * kSearchMaxPatterns words, zeroed
+    uint32_t *totals;        // np totals, written by the last tile
+    uint32_t *error;
+};
 
 cudaError_t launch_search(const SearchArgs &a, cudaStream_t st);
 

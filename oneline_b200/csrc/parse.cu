@@ -1,14 +1,15 @@
 // Kernel (a)+(b): newline scan fused with per-line classification.
 //
-// One pass over the text. Each CTA takes the next 16 KiB tile from a ticket
-// counter (so every predecessor tile is already running when a tile looks
-// back), loads it with 16-byte coalesced vector loads, finds its newlines with
-// byte SWAR, compacts their positions in order (warp popc scans), takes its
-// global line base from a single-pass decoupled look-back over tile newline
-// counts, and classifies every line that starts after one of its newlines while
-// the bytes are still in shared memory. A line that runs past the tile plus a
-// 256-byte halo is queued for a small fix-up kernel, which reads it from global
-// memory once the offsets array is complete.
+// One pass over the text. CTA b owns the 16 KiB tile b (blocks are dispatched in
+// index order, so the tiles a block looks back on are already running); it loads
+// the tile with 16-byte coalesced vector loads, finds its newlines with byte
+// SWAR, ranks them in position order with warp popc scans, publishes its newline
+// count at once, and then, while warp 0 runs the single-pass decoupled look-back
+// for the tile's global line base, warps 1..7 classify every line that starts
+// after one of the tile's newlines from shared memory. Results wait in
+// registers and are written, coalesced, once the base is known. A line that
+// runs past the tile plus a 256-byte halo is queued for a small fix-up kernel,
+// which reads it from global memory once the offsets array is complete.
 //
 // Replaces crates/oneline-gpu/src/scan.wgsl:20-237 (three passes + a host read
 // of the line count) and shader.wgsl:34-134 (one thread per line, byte loads
@@ -25,35 +26,80 @@ constexpr uint32_t PT_THREADS = 256;
 constexpr uint32_t PT_STEPS = 4;                          // 16-byte pieces per thread
 constexpr uint32_t PT_TILE = PT_THREADS * 16 * PT_STEPS;  // 16384
 constexpr uint32_t PT_HALO = 256;
+constexpr uint32_t PT_LIST = 1024;                        // newline positions listed per round
+constexpr uint32_t PT_WORKERS = PT_THREADS - 32;          // warps 1..7 classify, warp 0 looks back
+constexpr uint32_t PT_PER_WORKER = (PT_LIST + PT_WORKERS - 1) / PT_WORKERS;  // 10
 
 static_assert(PT_TILE == kParseTile && PT_HALO == kParseHalo, "tile geometry");
 
 struct ParseSmem {
-    alignas(16) uint8_t text[PT_TILE + PT_HALO];
-    uint16_t nl[PT_TILE];            // local newline positions, ascending
+    alignas(16) uint8_t text[PT_TILE + PT_HALO + 16];  // +16: word reads may run 3 bytes past
+    uint16_t nl[PT_LIST + 1];        // newline positions of the current round, ascending
     uint32_t warp_tot[PT_STEPS][8];  // newline count per (step, warp)
     uint32_t warp_base[PT_STEPS][8];
     uint32_t halo_first;             // first newline in the halo (local), or NONE
-    uint32_t tile;
     uint32_t nl_base;                // newlines before this tile
     uint32_t n_nl;                   // newlines in this tile
-    uint32_t max_depth;
 };
 
-__global__ void __launch_bounds__(PT_THREADS) parse_tiles_kernel(ParseArgs a) {
-    extern __shared__ __align__(16) uint8_t parse_smem_raw[];
-    ParseSmem &sm = *reinterpret_cast<ParseSmem *>(parse_smem_raw);
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+// Packed per-line result kept in registers until the tile's line base is known.
+constexpr uint32_t PK_NONE = 0xFFFFFFFFu;   // no line in this slot
+constexpr uint32_t PK_FIXUP = 0xFFFFFFFEu;  // offset only; the fix-up kernel classifies it
 
-    if (tid == 0) {
-        sm.tile = atomicAdd(&a.stats->ticket, 1u);
-        sm.halo_first = NONE;
-        sm.max_depth = 0;
+// 4 bytes of shared memory from any byte offset.
+__device__ __forceinline__ uint32_t lds4(const uint8_t *base, uint32_t off) {
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(base) + (off >> 2);
+    return __funnelshift_r(w[0], w[1], (off & 3) * 8);
+}
+
+// High bits of the bytes of w equal to '|' and to a blank (' ' or '\t').
+__device__ __forceinline__ uint32_t pipe_bits(uint32_t w) { return zero_bytes(w ^ 0x7C7C7C7Cu); }
+__device__ __forceinline__ uint32_t blank_bits(uint32_t w) {
+    return zero_bytes(w ^ 0x20202020u) | zero_bytes(w ^ 0x09090909u);
+}
+
+// parse_line (crates/oneline-simd/src/line.rs:8-44) for a line held in shared
+// memory at tile-local [s, e), e = its '\n' or the text end; the bytes from e
+// to e+3 are readable. Same rules as classify_line, four bytes per step.
+__device__ __forceinline__ uint32_t classify_smem(const uint8_t *t, uint32_t s, uint32_t e, uint32_t &depth_out,
+                                                  uint32_t &cs_out, uint32_t &eff_out) {
+    uint32_t eff = e;
+    while (eff > s && t[eff - 1] == '\r') eff--;
+    uint32_t c = s, depth = 0;
+    const bool piped = t[s] == '|' && s < eff;
+    for (;;) {
+        uint32_t w = lds4(t, c);
+        uint32_t hp = piped ? pipe_bits(w) : 0u;
+        uint32_t other = ~(hp | blank_bits(w)) & 0x80808080u;
+        if (other) {
+            uint32_t nb = (__ffs(other) - 8) >> 3;  // first byte that ends the prefix
+            depth += __popc(hp & ((1u << (8 * nb)) - 1u));
+            c += nb;
+            break;
+        }
+        depth += __popc(hp);
+        c += 4;
     }
-    __syncthreads();
-    const uint32_t tile = sm.tile;
+    // a prefix never runs into the '\r' / '\n' run, but a blank-only run may
+    // be followed by nothing: clamp to eff
+    if (c > eff) c = eff;
+    depth_out = depth;
+    cs_out = c;
+    eff_out = eff;
+    if (c >= eff) return KIND_BLANK;
+    uint32_t n = eff - c;
+    uint32_t w = lds4(t, c);
+    return classify3((uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), n);
+}
+
+__global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a) {
+    __shared__ ParseSmem sm;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t tile = blockIdx.x;
     const uint64_t t0 = (uint64_t)tile * PT_TILE;
     const uint64_t N = a.text_len;
+    // bytes of this tile (and halo) that belong to the text
+    const uint32_t valid = N - t0 >= PT_TILE + PT_HALO ? PT_TILE + PT_HALO : (uint32_t)(N - t0);
 
     // 1. Coalesced 16-byte loads: step k covers [t0 + k*4096, +4096), lane-major.
     uint4 v[PT_STEPS];
@@ -61,47 +107,75 @@ __global__ void __launch_bounds__(PT_THREADS) parse_tiles_kernel(ParseArgs a) {
     for (uint32_t k = 0; k < PT_STEPS; k++) v[k] = ld_stream16(a.text + t0 + k * 4096 + tid * 16);
     uint4 vh = make_uint4(0, 0, 0, 0);
     if (tid < PT_HALO / 16) vh = ld_stream16(a.text + t0 + PT_TILE + tid * 16);
-
+    if (tid == 0) {
+        sm.halo_first = NONE;
+        *reinterpret_cast<uint4 *>(&sm.text[PT_TILE + PT_HALO]) = make_uint4(0, 0, 0, 0);
+    }
 #pragma unroll
     for (uint32_t k = 0; k < PT_STEPS; k++) *reinterpret_cast<uint4 *>(&sm.text[k * 4096 + tid * 16]) = v[k];
     if (tid < PT_HALO / 16) *reinterpret_cast<uint4 *>(&sm.text[PT_TILE + tid * 16]) = vh;
 
-    // 2. Newline masks, only for positions < N.
+    // 2. Newline bits: z[k][i] has the high bit of each '\n' byte of word i of
+    //    piece k (exact SWAR test; bytes at or past the text end cleared).
     const uint32_t NL4 = 0x0A0A0A0Au;
-    uint32_t m[PT_STEPS];
+    uint32_t z[PT_STEPS][4];
+    uint32_t cnt[PT_STEPS];
 #pragma unroll
     for (uint32_t k = 0; k < PT_STEPS; k++) {
-        uint64_t p0 = t0 + k * 4096 + tid * 16;
-        uint32_t mk = eq_mask16(v[k], NL4);
-        if (p0 + 16 > N) mk &= p0 >= N ? 0u : ((1u << (uint32_t)(N - p0)) - 1u);
-        m[k] = mk;
+        const uint32_t lo = k * 4096 + tid * 16;
+        z[k][0] = zero_bytes(v[k].x ^ NL4);
+        z[k][1] = zero_bytes(v[k].y ^ NL4);
+        z[k][2] = zero_bytes(v[k].z ^ NL4);
+        z[k][3] = zero_bytes(v[k].w ^ NL4);
+        if (lo + 16 > valid) {
+#pragma unroll
+            for (uint32_t i = 0; i < 4; i++) {
+                uint32_t b0 = lo + 4 * i;  // bytes b0..b0+3; keep those < valid
+                uint32_t keep = b0 >= valid ? 0u : (valid - b0 >= 4 ? 4u : valid - b0);
+                z[k][i] &= keep == 4 ? 0xFFFFFFFFu : ((1u << (8 * keep)) - 1u);
+            }
+        }
+        cnt[k] = __popc(z[k][0]) + __popc(z[k][1]) + __popc(z[k][2]) + __popc(z[k][3]);
     }
+    // Ranks within the warp: steps (0,1) and (2,3) packed in 16-bit fields.
+    uint32_t c01 = cnt[0] | (cnt[1] << 16), c23 = cnt[2] | (cnt[3] << 16);
+    uint32_t i01 = c01, i23 = c23;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t1 = __shfl_up_sync(0xFFFFFFFFu, i01, o);
+        uint32_t t2 = __shfl_up_sync(0xFFFFFFFFu, i23, o);
+        if ((int)lane >= o) {
+            i01 += t1;
+            i23 += t2;
+        }
+    }
+    const uint32_t r01 = i01 - c01, r23 = i23 - c23;
+    if (lane == 31) {
+        sm.warp_tot[0][warp] = i01 & 0xFFFF;
+        sm.warp_tot[1][warp] = i01 >> 16;
+        sm.warp_tot[2][warp] = i23 & 0xFFFF;
+        sm.warp_tot[3][warp] = i23 >> 16;
+    }
+    __syncthreads();  // (a) halo_first initialised, warp totals visible
     if (tid < PT_HALO / 16) {
-        uint64_t p0 = t0 + PT_TILE + tid * 16;
-        uint32_t mh = eq_mask16(vh, NL4);
-        if (p0 + 16 > N) mh &= p0 >= N ? 0u : ((1u << (uint32_t)(N - p0)) - 1u);
-        uint32_t first = mh ? PT_TILE + tid * 16 + __ffs(mh) - 1 : NONE;
-        // lanes 0..15 of warp 0
+        const uint32_t lo = PT_TILE + tid * 16;
+        uint32_t first = NONE;
+        uint32_t hw[4] = {vh.x, vh.y, vh.z, vh.w};
+#pragma unroll
+        for (int i = 3; i >= 0; i--) {
+            uint32_t zz = zero_bytes(hw[i] ^ NL4);
+            uint32_t b0 = lo + 4 * i;
+            uint32_t keep = b0 >= valid ? 0u : (valid - b0 >= 4 ? 4u : valid - b0);
+            zz &= keep == 4 ? 0xFFFFFFFFu : ((1u << (8 * keep)) - 1u);
+            if (zz) first = b0 + ((__ffs(zz) - 8) >> 3);
+        }
         for (int o = 8; o > 0; o >>= 1) first = min(first, __shfl_xor_sync(0x0000FFFFu, first, o));
         if (tid == 0) sm.halo_first = first;
     }
-
-    // 3. Per-(step, warp) exclusive scans of the newline counts.
-    uint32_t rank[PT_STEPS];
-#pragma unroll
-    for (uint32_t k = 0; k < PT_STEPS; k++) {
-        uint32_t c = __popc(m[k]), inc = c;
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
-            if ((int)lane >= o) inc += t;
-        }
-        rank[k] = inc - c;
-        if (lane == 31) sm.warp_tot[k][warp] = inc;
-    }
-    __syncthreads();
-    if (warp == 0) {
+    if (warp == 1) {
         // 32 (step, warp) totals in position order: index = k*8 + w.
         uint32_t c = sm.warp_tot[lane >> 3][lane & 7], inc = c;
+#pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
             if ((int)lane >= o) inc += t;
@@ -110,76 +184,103 @@ __global__ void __launch_bounds__(PT_THREADS) parse_tiles_kernel(ParseArgs a) {
         uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
         if (lane == 0) {
             sm.n_nl = total;
-            // Publish the aggregate (tile 0 publishes its prefix at once).
+            // Publish the aggregate at once (tile 0 publishes its prefix).
             st_relaxed_u64(a.tile_status + tile, (uint64_t)total | (tile == 0 ? LB_PREFIX : LB_AGGREGATE));
         }
     }
-    __syncthreads();
+    __syncthreads();  // (b) bases and n_nl visible
 
-    // 4. Ordered list of newline positions.
-#pragma unroll
-    for (uint32_t k = 0; k < PT_STEPS; k++) {
-        uint32_t r = sm.warp_base[k][warp] + rank[k];
-        uint32_t mk = m[k];
-        while (mk) {
-            uint32_t b = __ffs(mk) - 1;
-            mk &= mk - 1;
-            sm.nl[r++] = (uint16_t)(k * 4096 + tid * 16 + b);
-        }
-    }
-
-    // 5. Look-back for the number of newlines before this tile.
-    if (warp == 0) {
-        uint32_t base = tile == 0 ? 0u : lb_sum_exclusive(a.tile_status, tile, &a.stats->error);
-        if (lane == 0) {
-            sm.nl_base = base;
-            if (tile != 0) st_relaxed_u64(a.tile_status + tile, (uint64_t)(base + sm.n_nl) | LB_PREFIX);
-            if (tile == a.n_tiles - 1) {
-                // L = 1 + newlines before the last byte.
-                uint32_t total_nl = base + sm.n_nl;
-                uint32_t last_is_nl = a.text[N - 1] == '\n';
-                a.stats->line_count = 1u + total_nl - last_is_nl;
-            }
-        }
-    }
-    __syncthreads();
-
-    // 6. Classify the lines that start in this tile (after one of its newlines,
-    //    plus line 0 for tile 0).
     const uint32_t n_nl = sm.n_nl, off = tile == 0 ? 1u : 0u;
     const uint32_t n_lines = n_nl + off;
-    const uint64_t stage_end = t0 + PT_TILE + PT_HALO;
     const uint32_t halo_first = sm.halo_first;
     uint32_t my_max = 0;
-    auto at = [&](uint32_t pos) -> uint8_t { return sm.text[pos - t0]; };
-    for (uint32_t j = tid; j < n_lines; j += PT_THREADS) {
-        int32_t q = (int32_t)j - (int32_t)off;  // newline that precedes the line (-1: none)
-        uint64_t s = q < 0 ? 0 : t0 + sm.nl[q] + 1;
-        if (s >= N) continue;  // the final '\n' starts no line
-        uint32_t idx = sm.nl_base + j + 1 - off;
-        uint64_t e;
-        if ((uint32_t)(q + 1) < n_nl) e = t0 + sm.nl[q + 1];
-        else if (halo_first != NONE) e = t0 + halo_first;
-        else if (N <= stage_end) e = N;
-        else {
-            // Runs past the halo: classified by the fix-up kernel.
-            uint32_t slot = atomicAdd(&a.stats->fixup_count, 1u);
-            if (slot < a.fixup_cap) a.fixup[slot] = make_uint2(idx, (uint32_t)s);
-            else atomicOr(&a.stats->error, OL_DEVERR_FIXUP);
-            if (idx < a.line_cap) a.offsets[idx] = (uint32_t)s;
-            else atomicOr(&a.stats->error, OL_DEVERR_CAPACITY);
-            continue;
+    bool base_known = false;
+
+    // Lines are classified in rounds of PT_LIST (one round unless the tile
+    // holds more than 1024 newlines): list the round's newline positions, then
+    // warps 1..7 classify while warp 0 runs the look-back (first round only).
+    for (uint32_t r0 = 0; r0 < n_lines || (r0 == 0 && !base_known); r0 += PT_LIST) {
+        const int32_t w0 = (int32_t)r0 - (int32_t)off;  // rank of nl[0]
+#pragma unroll
+        for (uint32_t k = 0; k < PT_STEPS; k++) {
+            uint32_t rr = (k & 1) ? ((k < 2 ? r01 : r23) >> 16) : ((k < 2 ? r01 : r23) & 0xFFFF);
+            int32_t rk = (int32_t)(sm.warp_base[k][warp] + rr) - w0;
+            if (rk > (int32_t)PT_LIST) continue;
+#pragma unroll
+            for (uint32_t i = 0; i < 4; i++) {
+                uint32_t zz = z[k][i];
+                while (zz) {
+                    uint32_t b = (__ffs(zz) - 8) >> 3;
+                    zz &= zz - 1;
+                    if (rk >= 0 && rk <= (int32_t)PT_LIST) sm.nl[rk] = (uint16_t)(k * 4096 + tid * 16 + 4 * i + b);
+                    rk++;
+                }
+            }
         }
-        FlatNode nd = classify_line((uint32_t)s, (uint32_t)e, at);
-        if (idx >= a.line_cap) {
-            atomicOr(&a.stats->error, OL_DEVERR_CAPACITY);
-            continue;
+        __syncthreads();  // (c) list ready
+
+        uint32_t res_off[PT_PER_WORKER], res_pk[PT_PER_WORKER];
+        if (warp == 0) {
+            if (!base_known) {
+                uint32_t nl_base = tile == 0 ? 0u : lb_sum_exclusive(a.tile_status, tile, &a.stats->error);
+                if (lane == 0) {
+                    sm.nl_base = nl_base;
+                    if (tile != 0) st_relaxed_u64(a.tile_status + tile, (uint64_t)(nl_base + n_nl) | LB_PREFIX);
+                    if (tile == a.n_tiles - 1) {
+                        uint32_t total_nl = nl_base + n_nl;  // L = 1 + newlines before the last byte
+                        a.stats->line_count = 1u + total_nl - (a.text[N - 1] == '\n');
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (uint32_t i = 0; i < PT_PER_WORKER; i++) {
+                uint32_t j = r0 + (tid - 32) + i * PT_WORKERS;
+                res_pk[i] = PK_NONE;
+                res_off[i] = 0;
+                if (j >= n_lines || j >= r0 + PT_LIST) continue;
+                int32_t q = (int32_t)j - (int32_t)off;  // newline that precedes the line (-1: none)
+                uint32_t s = q < 0 ? 0u : sm.nl[q - w0] + 1u;  // tile-local
+                if (s >= valid) continue;  // the final '\n' starts no line
+                res_off[i] = (uint32_t)t0 + s;
+                uint32_t e;
+                if ((uint32_t)(q + 1) < n_nl) e = sm.nl[q + 1 - w0];
+                else if (halo_first != NONE) e = halo_first;
+                else if (valid < PT_TILE + PT_HALO) e = valid;  // the text ends in the staged bytes
+                else {
+                    res_pk[i] = PK_FIXUP;  // runs past the halo
+                    continue;
+                }
+                uint32_t depth, cs, eff;
+                uint32_t kind = classify_smem(sm.text, s, e, depth, cs, eff);
+                res_pk[i] = kind | (min(depth, 255u) << 8);
+                if (kind != KIND_BLANK) my_max = max(my_max, depth);
+            }
         }
-        a.offsets[idx] = (uint32_t)s;
-        a.kinds[idx] = (uint8_t)nd.kind;
-        a.depth8[idx] = (uint8_t)min(nd.depth, 255u);
-        if (nd.kind != KIND_BLANK) my_max = max(my_max, nd.depth);
-        if (a.nodes) a.nodes[idx] = nd;
+        __syncthreads();  // (d) base known; the list may be rewritten
+        base_known = true;
+        const uint32_t nl_base = sm.nl_base;
+        if (warp != 0) {
+#pragma unroll
+            for (uint32_t i = 0; i < PT_PER_WORKER; i++) {
+                if (res_pk[i] == PK_NONE) continue;
+                uint32_t j = r0 + (tid - 32) + i * PT_WORKERS;
+                uint32_t idx = nl_base + j + 1 - off;
+                if (idx >= a.line_cap) {
+                    atomicOr(&a.stats->error, OL_DEVERR_CAPACITY);
+                    continue;
+                }
+                a.offsets[idx] = res_off[i];
+                if (res_pk[i] == PK_FIXUP) {
+                    uint32_t slot = atomicAdd(&a.stats->fixup_count, 1u);
+                    if (slot < a.fixup_cap) a.fixup[slot] = make_uint2(idx, res_off[i]);
+                    else atomicOr(&a.stats->error, OL_DEVERR_FIXUP);
+                    continue;
+                }
+                a.kinds[idx] = (uint8_t)(res_pk[i] & 0xFF);
+                a.depth8[idx] = (uint8_t)(res_pk[i] >> 8);
+            }
+        }
     }
     for (int o = 16; o > 0; o >>= 1) my_max = max(my_max, __shfl_xor_sync(0xFFFFFFFFu, my_max, o));
     if (lane == 0 && my_max) atomicMax(&a.stats->max_content_depth, my_max);
@@ -206,7 +307,6 @@ __global__ void parse_fixup_kernel(ParseArgs a) {
         if (idx >= a.line_cap) continue;
         a.kinds[idx] = (uint8_t)nd.kind;
         a.depth8[idx] = (uint8_t)min(nd.depth, 255u);
-        if (a.nodes) a.nodes[idx] = nd;
         if (nd.kind != KIND_BLANK) atomicMax(&a.stats->max_content_depth, nd.depth);
     }
 }
@@ -230,10 +330,7 @@ __global__ void classify_lines_kernel(const uint8_t *__restrict__ text, uint64_t
 
 cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st) {
     if (a.n_tiles == 0) return cudaSuccess;
-    cudaError_t e0 = cudaFuncSetAttribute(parse_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)sizeof(ParseSmem));
-    if (e0 != cudaSuccess) return e0;
-    parse_tiles_kernel<<<a.n_tiles, PT_THREADS, sizeof(ParseSmem), st>>>(a);
+    parse_tiles_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     uint32_t blocks = a.fixup_cap < 64 ? 8 : 64;

@@ -108,6 +108,7 @@ extern "C" ol_status ol_ctx_create(int32_t device, ol_ctx **out) {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
     e = cudaMallocAsync((void **)&c->counters, sizeof(CtxCounters), c->stream);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pat_done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&c->host_counters, sizeof(CtxCounters));
     for (int i = 0; i < kRingSlots && e == cudaSuccess; i++) {
         e = cudaMallocHost((void **)&c->ring[i], kRingBytes);
@@ -134,6 +135,8 @@ extern "C" void ol_ctx_destroy(ol_ctx *ctx) {
     if (ctx->counters) cudaFreeAsync(ctx->counters, ctx->stream);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->host_counters) cudaFreeHost(ctx->host_counters);
+    if (ctx->pat_host) cudaFreeHost(ctx->pat_host);
+    if (ctx->pat_done) cudaEventDestroy(ctx->pat_done);
     for (int i = 0; i < kRingSlots; i++) {
         if (ctx->ring[i]) cudaFreeHost(ctx->ring[i]);
         if (ctx->ring_done[i]) cudaEventDestroy(ctx->ring_done[i]);
@@ -184,7 +187,7 @@ cudaError_t h2d(ol_ctx *ctx, uint8_t *dev, const uint8_t *host, uint64_t len) {
 }
 
 // Enqueues the parse of doc's resident text into its buffers.
-cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d, FlatNode *nodes) {
+cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d) {
     cudaStream_t st = ctx->stream;
     cudaError_t e;
     uint32_t n_tiles = parse_tiles(d->text_len);
@@ -200,7 +203,6 @@ cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d, FlatNode *nodes) {
     a.offsets = d->offsets;
     a.kinds = d->kinds;
     a.depth8 = d->depth8;
-    a.nodes = nodes;
     a.line_cap = d->line_cap;
     a.fixup = d->fixup;
     a.fixup_cap = n_tiles;
@@ -225,20 +227,14 @@ ol_status alloc_lines(ol_ctx *ctx, ol_doc *d, uint64_t cap_lines) {
 }
 
 // Runs the parse (with one exact-size retry when the estimate was too low),
-// waits, and records the line count. nodes (device, optional) gets FlatNodes;
-// nodes_cap must then be >= the capacity passed in.
+// waits, and records the line count. With nodes_out, the 16-byte nodes are
+// materialised into ctx->scratch_c as well.
 ol_status parse_doc(ol_ctx *ctx, ol_doc *d, uint64_t est_lines, FlatNode **nodes_out) {
     cudaStream_t st = ctx->stream;
     for (int attempt = 0; attempt < 2; attempt++) {
         ol_status s = alloc_lines(ctx, d, est_lines);
         if (s != OL_OK) return s;
-        FlatNode *nodes = nullptr;
-        if (nodes_out) {
-            cudaError_t e = ctx->scratch_c.reserve((size_t)d->line_cap * sizeof(FlatNode), st);
-            if (e != cudaSuccess) return ctx_cuda(ctx, e, "allocate nodes");
-            nodes = (FlatNode *)ctx->scratch_c.ptr;
-        }
-        cudaError_t e = enqueue_parse(ctx, d, nodes);
+        cudaError_t e = enqueue_parse(ctx, d);
         if (e == cudaSuccess) e = cudaMemcpyAsync(&d->host_stats, d->stats, sizeof(DocStats), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "parse");
@@ -251,7 +247,14 @@ ol_status parse_doc(ol_ctx *ctx, ol_doc *d, uint64_t est_lines, FlatNode **nodes
         }
         d->line_count = hs.line_count;
         d->max_depth = hs.max_content_depth;
-        if (nodes_out) *nodes_out = nodes;
+        if (nodes_out) {
+            e = ctx->scratch_c.reserve((size_t)d->line_cap * sizeof(FlatNode), st);
+            if (e == cudaSuccess)
+                e = launch_classify_lines(d->text, d->text_len, d->offsets, d->line_count, (FlatNode *)ctx->scratch_c.ptr,
+                                          nullptr, st);
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "materialise nodes");
+            *nodes_out = (FlatNode *)ctx->scratch_c.ptr;
+        }
         return OL_OK;
     }
     return ctx_fail(ctx, OL_ERR_CUDA, "parse: line capacity retry failed");
@@ -352,7 +355,7 @@ extern "C" ol_status ol_doc_reparse_async(ol_ctx *ctx, ol_doc *d) {
     if (d->text_len == 0) return OL_OK;
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
-    return ctx_cuda(ctx, enqueue_parse(ctx, d, nullptr), "reparse");
+    return ctx_cuda(ctx, enqueue_parse(ctx, d), "reparse");
 }
 
 static ol_status read_array(ol_ctx *ctx, const ol_doc *d, void *out, const void *src, size_t elem, uint64_t cap) {

@@ -48,6 +48,9 @@ struct ol_ctx {
     ol::DevBuf pattern_dev;
     ol::CtxCounters *counters = nullptr;
     ol::CtxCounters *host_counters = nullptr;  // pinned
+    uint8_t *pat_host = nullptr;  // pinned staging for pattern bytes
+    size_t pat_host_bytes = 0;
+    cudaEvent_t pat_done = nullptr;
     uint8_t *ring[ol::kRingSlots] = {nullptr};
     cudaEvent_t ring_done[ol::kRingSlots] = {nullptr};
 };

@@ -1,11 +1,13 @@
 // C ABI for substring search (GpuParser::search_document / search_raw,
-// crates/oneline-gpu/src/search.rs:32-140).
+// crates/oneline-gpu/src/search.rs:32-140), plus the batched form that
+// searches up to eight patterns per pass over the text.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "runtime.h"
 
@@ -13,55 +15,128 @@ using namespace ol;
 
 namespace {
 
-// Enqueues one search over doc; results stay on the device.
-cudaError_t enqueue_search(ol_ctx *ctx, const ol_doc *d, const uint8_t *pattern, uint32_t m, uint32_t max_out,
-                           uint32_t *d_total, uint32_t *d_out, uint32_t *d_ticket, uint32_t *d_error) {
+uint32_t halo_for(uint32_t m) { return ((m > 0 ? m - 1 : 0) + 15u) & ~15u; }
+
+// Enqueues searches of n patterns over doc, at most 8 per launch (longer than
+// the staged limit: one per launch). Results stay on the device: d_totals[i]
+// and d_outs[i]. Pattern bytes are copied to device memory first.
+cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pats, const uint32_t *lens, uint32_t n,
+                          const uint32_t *max_out, uint32_t *d_totals, uint32_t *const *d_outs, uint32_t *d_error) {
     cudaStream_t st = ctx->stream;
     uint32_t n_tiles = (uint32_t)((d->text_len + kSearchTile - 1) / kSearchTile);
-    cudaError_t e = ctx->scratch_a.reserve((size_t)n_tiles * 8, st);
-    if (e == cudaSuccess) e = ctx->pattern_dev.reserve(std::max<size_t>(m, 16), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->scratch_a.ptr, 0, (size_t)n_tiles * 8, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_ticket, 0, 4, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_total, 0, 4, st);
-    // The pattern travels by value through a pageable copy: stream ordered, and
-    // the call returns only after the source has been read.
-    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->pattern_dev.ptr, pattern, m, cudaMemcpyHostToDevice, st);
+    size_t total_bytes = 0;
+    for (uint32_t i = 0; i < n; i++) total_bytes += (lens[i] + 15) & ~15u;
+    cudaError_t e = ctx->pattern_dev.reserve(std::max<size_t>(total_bytes, 16), st);
+    if (e == cudaSuccess) e = ctx->scratch_a.reserve((size_t)n_tiles * kSearchMaxPatterns * 8, st);
     if (e != cudaSuccess) return e;
-    SearchArgs a{};
-    a.text = d->text;
-    a.text_len = d->text_len;
-    a.pattern = (const uint8_t *)ctx->pattern_dev.ptr;
-    a.pat_len = m;
-    a.n_tiles = n_tiles;
-    a.tile_status = (uint64_t *)ctx->scratch_a.ptr;
-    a.ticket = d_ticket;
-    a.total = d_total;
-    a.error = d_error;
-    a.out = d_out;
-    a.max_out = max_out;
-    return launch_search(a, st);
+    // Patterns travel through pinned host staging so the copy is truly async
+    // and the caller's buffers may be reused once this call returns.
+    if (ctx->pat_host_bytes < total_bytes) {
+        if (ctx->pat_host) {
+            cudaStreamSynchronize(st);
+            cudaFreeHost(ctx->pat_host);
+        }
+        ctx->pat_host = nullptr;
+        ctx->pat_host_bytes = 0;
+        if ((e = cudaMallocHost((void **)&ctx->pat_host, std::max<size_t>(total_bytes, 4096))) != cudaSuccess) return e;
+        ctx->pat_host_bytes = std::max<size_t>(total_bytes, 4096);
+    } else {
+        // the previous pattern upload must have left the staging buffer
+        if ((e = cudaEventSynchronize(ctx->pat_done)) != cudaSuccess) return e;
+    }
+    std::vector<size_t> at(n);
+    size_t w = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        at[i] = w;
+        memcpy(ctx->pat_host + w, pats[i], lens[i]);
+        w += (lens[i] + 15) & ~15u;
+    }
+    uint8_t *dpat = (uint8_t *)ctx->pattern_dev.ptr;
+    if ((e = cudaMemcpyAsync(dpat, ctx->pat_host, std::max<size_t>(w, 1), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(ctx->pat_done, st)) != cudaSuccess) return e;
+
+    uint32_t i = 0;
+    while (i < n) {
+        SearchArgs a{};
+        a.text = d->text;
+        a.text_len = d->text_len;
+        a.n_tiles = n_tiles;
+        a.tile_status = (uint64_t *)ctx->scratch_a.ptr;
+        a.error = d_error;
+        uint32_t halo = 0;
+        bool alone = halo_for(lens[i]) > kSearchMaxStagedPattern;
+        uint32_t first = i;
+        while (i < n && a.np < kSearchMaxPatterns) {
+            bool long_pat = halo_for(lens[i]) > kSearchMaxStagedPattern;
+            if (a.np > 0 && (alone || long_pat)) break;
+            a.pat[a.np] = dpat + at[i];
+            a.pat_len[a.np] = lens[i];
+            a.out[a.np] = d_outs[i];
+            a.max_out[a.np] = max_out[i];
+            halo = std::max(halo, halo_for(lens[i]));
+            a.np++;
+            i++;
+            if (alone) break;
+        }
+        a.halo = halo;
+        a.totals = d_totals + first;
+        if ((e = cudaMemsetAsync(a.tile_status, 0, (size_t)n_tiles * kSearchMaxPatterns * 8, st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(a.totals, 0, (size_t)a.np * 4, st)) != cudaSuccess) return e;
+        if ((e = launch_search(a, st)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
-ol_status search_doc(ol_ctx *ctx, const ol_doc *d, const uint8_t *pattern, uint32_t m, uint32_t max_matches,
-                     uint32_t *total, uint32_t *out) {
-    *total = 0;
-    if (d->text_len == 0 || d->text_len < m) return OL_OK;
+// Blocking multi-pattern search into host buffers.
+ol_status search_multi_host(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pats, const uint32_t *lens, uint32_t n,
+                            const uint32_t *max_matches, uint32_t *totals, uint32_t *const *outs) {
+    for (uint32_t i = 0; i < n; i++) totals[i] = 0;
+    if (d->text_len == 0 || n == 0) return OL_OK;
     cudaStream_t st = ctx->stream;
-    cudaError_t e = ctx->search_out.reserve((size_t)std::max<uint32_t>(max_matches, 1) * 4, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(&ctx->counters->error, 0, 4, st);
-    if (e == cudaSuccess)
-        e = enqueue_search(ctx, d, pattern, m, max_matches, &ctx->counters->total, (uint32_t *)ctx->search_out.ptr,
-                           &ctx->counters->ticket, &ctx->counters->error);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->host_counters, ctx->counters, sizeof(CtxCounters), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    // Patterns longer than the text cannot match: skip them.
+    std::vector<uint32_t> idx;
+    size_t out_words = 0;
+    for (uint32_t i = 0; i < n; i++)
+        if (lens[i] <= d->text_len) {
+            idx.push_back(i);
+            out_words += std::max<uint32_t>(max_matches[i], 1);
+        }
+    if (idx.empty()) return OL_OK;
+    cudaError_t e = ctx->search_out.reserve(out_words * 4 + 64 * 4, st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "search");
-    if (ctx->host_counters->error & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "search: a look-back wait timed out");
-    *total = ctx->host_counters->total;
-    uint32_t n = std::min(*total, max_matches);
-    if (n > 0) {
-        e = cudaMemcpyAsync(out, ctx->search_out.ptr, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
+    uint32_t *dev = (uint32_t *)ctx->search_out.ptr;
+    uint32_t *d_totals = dev;  // 64 slots
+    std::vector<const uint8_t *> p2;
+    std::vector<uint32_t> l2, m2;
+    std::vector<uint32_t *> o2;
+    size_t w = 64;
+    for (uint32_t i : idx) {
+        p2.push_back(pats[i]);
+        l2.push_back(lens[i]);
+        m2.push_back(max_matches[i]);
+        o2.push_back(dev + w);
+        w += std::max<uint32_t>(max_matches[i], 1);
+    }
+    for (size_t c = 0; c < idx.size(); c += 64) {
+        uint32_t cn = (uint32_t)std::min<size_t>(64, idx.size() - c);
+        e = cudaMemsetAsync(&ctx->counters->error, 0, 4, st);
+        if (e == cudaSuccess)
+            e = enqueue_multi(ctx, d, p2.data() + c, l2.data() + c, cn, m2.data() + c, d_totals, o2.data() + c,
+                              &ctx->counters->error);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->host_counters, ctx->counters, sizeof(CtxCounters), cudaMemcpyDeviceToHost, st);
+        uint32_t tot_h[64];
+        if (e == cudaSuccess) e = cudaMemcpyAsync(tot_h, d_totals, cn * 4, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return ctx_cuda(ctx, e, "search download");
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "search");
+        if (ctx->host_counters->error & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "search: a look-back wait timed out");
+        for (uint32_t j = 0; j < cn; j++) {
+            uint32_t i = idx[c + j];
+            totals[i] = tot_h[j];
+            uint32_t k = std::min(tot_h[j], max_matches[i]);
+            if (k > 0 && (e = cudaMemcpyAsync(outs[i], o2[c + j], (size_t)k * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+                return ctx_cuda(ctx, e, "search download");
+        }
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx_cuda(ctx, e, "search download");
     }
     return OL_OK;
 }
@@ -74,7 +149,19 @@ extern "C" ol_status ol_search(ol_ctx *ctx, const ol_doc *d, const uint8_t *patt
     if (pat_len == 0 || !pattern) return ctx_fail(ctx, OL_ERR_BAD_PATTERN, "pattern must not be empty");
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
-    return search_doc(ctx, d, pattern, pat_len, max_matches, total, out);
+    return search_multi_host(ctx, d, &pattern, &pat_len, 1, &max_matches, total, &out);
+}
+
+extern "C" ol_status ol_search_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *patterns, const uint32_t *lens,
+                                     uint32_t n, const uint32_t *max_matches, uint32_t *totals, uint32_t *const *outs) {
+    if (!ctx || !d || (n && (!patterns || !lens || !max_matches || !totals || !outs))) return OL_ERR_INVALID_ARG;
+    for (uint32_t i = 0; i < n; i++) {
+        if (lens[i] == 0 || !patterns[i]) return ctx_fail(ctx, OL_ERR_BAD_PATTERN, "pattern " + std::to_string(i) + " is empty");
+        if (max_matches[i] && !outs[i]) return OL_ERR_INVALID_ARG;
+    }
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return search_multi_host(ctx, d, patterns, lens, n, max_matches, totals, outs);
 }
 
 extern "C" ol_status ol_search_raw(ol_ctx *ctx, const uint8_t *text, uint64_t len, const uint8_t *pattern, uint32_t pat_len,
@@ -89,20 +176,53 @@ extern "C" ol_status ol_search_raw(ol_ctx *ctx, const uint8_t *text, uint64_t le
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
     ol_status s = new_text_doc(ctx, text, len, &d);
-    if (s == OL_OK) s = search_doc(ctx, d, pattern, pat_len, max_matches, total, out);
+    if (s == OL_OK) s = search_multi_host(ctx, d, &pattern, &pat_len, 1, &max_matches, total, &out);
     ol_doc_free(d);
     return s;
 }
 
 extern "C" ol_status ol_search_async(ol_ctx *ctx, const ol_doc *d, const uint8_t *pattern, uint32_t pat_len,
                                      uint32_t max_matches, uint32_t *d_total, uint32_t *d_out) {
-    if (!ctx || !d || !d_total || (max_matches && !d_out)) return OL_ERR_INVALID_ARG;
-    if (pat_len == 0 || !pattern) return ctx_fail(ctx, OL_ERR_BAD_PATTERN, "pattern must not be empty");
+    return ol_search_multi_async(ctx, d, &pattern, &pat_len, 1, &max_matches, d_total, &d_out);
+}
+
+extern "C" ol_status ol_search_multi_async(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *patterns, const uint32_t *lens,
+                                           uint32_t n, const uint32_t *max_matches, uint32_t *d_totals, uint32_t *const *d_outs) {
+    if (!ctx || !d || (n && (!patterns || !lens || !max_matches || !d_totals || !d_outs))) return OL_ERR_INVALID_ARG;
+    for (uint32_t i = 0; i < n; i++) {
+        if (lens[i] == 0 || !patterns[i]) return ctx_fail(ctx, OL_ERR_BAD_PATTERN, "pattern " + std::to_string(i) + " is empty");
+        if (max_matches[i] && !d_outs[i]) return OL_ERR_INVALID_ARG;
+    }
+    if (n == 0) return OL_OK;
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
-    if (d->text_len < pat_len) return ctx_cuda(ctx, cudaMemsetAsync(d_total, 0, 4, ctx->stream), "search");
-    return ctx_cuda(ctx,
-                    enqueue_search(ctx, d, pattern, pat_len, max_matches, d_total, d_out, &ctx->counters->ticket,
-                                   &ctx->counters->error),
-                    "search");
+    cudaStream_t st = ctx->stream;
+    // Patterns that cannot fit in the text report 0 and are not launched.
+    std::vector<const uint8_t *> p2;
+    std::vector<uint32_t> l2, m2, map;
+    std::vector<uint32_t *> o2;
+    for (uint32_t i = 0; i < n; i++) {
+        if (lens[i] > d->text_len) {
+            cudaError_t e = cudaMemsetAsync(d_totals + i, 0, 4, st);
+            if (e != cudaSuccess) return ctx_cuda(ctx, e, "search");
+            continue;
+        }
+        p2.push_back(patterns[i]);
+        l2.push_back(lens[i]);
+        m2.push_back(max_matches[i]);
+        o2.push_back(d_outs[i]);
+        map.push_back(i);
+    }
+    // Launches write totals of consecutive patterns: run maximal runs of kept
+    // patterns whose indices are consecutive.
+    size_t a = 0;
+    while (a < map.size()) {
+        size_t b = a + 1;
+        while (b < map.size() && map[b] == map[b - 1] + 1) b++;
+        cudaError_t e = enqueue_multi(ctx, d, p2.data() + a, l2.data() + a, (uint32_t)(b - a), m2.data() + a,
+                                      d_totals + map[a], o2.data() + a, &ctx->counters->error);
+        if (e != cudaSuccess) return ctx_cuda(ctx, e, "search");
+        a = b;
+    }
+    return OL_OK;
 }

@@ -16,6 +16,7 @@ library; there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -72,6 +73,7 @@ class GpuDocument:
         self._parser = parser
         self._h = handle
         self._source = source
+        parser._children.add(self)
 
     @property
     def handle(self) -> int:
@@ -105,9 +107,11 @@ class GpuDocument:
         return out[:n]
 
     def free(self) -> None:
-        if self._h:
+        # A document never outlives its parser's context: GpuParser.close()
+        # frees the documents and trees it still owns before destroying it.
+        if self._h and self._parser._ctx:
             _lib.load().ol_doc_free(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:
@@ -122,6 +126,7 @@ class GpuTree:
     def __init__(self, parser: "GpuParser", handle: int):
         self._parser = parser
         self._h = handle
+        parser._children.add(self)
 
     @property
     def handle(self) -> int:
@@ -135,9 +140,9 @@ class GpuTree:
         return h
 
     def free(self) -> None:
-        if self._h:
+        if self._h and self._parser._ctx:
             _lib.load().ol_tree_free(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:
@@ -156,6 +161,7 @@ class GpuParser:
         if st != 0:
             raise OnelineError(st, f"cannot create a CUDA context on device {device}")
         self._ctx = h.value
+        self._children = weakref.WeakSet()  # documents and trees that hold device memory
 
     @classmethod
     def new(cls, device: int = 0) -> "GpuParser":
@@ -163,6 +169,8 @@ class GpuParser:
 
     def close(self) -> None:
         if getattr(self, "_ctx", None):
+            for child in list(self._children):
+                child.free()
             _lib.load().ol_ctx_destroy(self._ctx)
             self._ctx = None
 
@@ -294,6 +302,25 @@ class GpuParser:
                                     ctypes.byref(total), out.ctypes.data), self._ctx)
         k = min(total.value, max_matches)
         return SearchResult(total.value, out[:k].copy())
+
+    def search_document_multi(self, doc: GpuDocument, patterns, max_matches) -> list:
+        """Several patterns at once (up to eight share each pass over the text).
+        `max_matches` is one int for all or one per pattern. Any pattern length."""
+        pats = [self._check_pattern(p, None) for p in patterns]
+        n = len(pats)
+        if n == 0:
+            return []
+        maxes = [int(max_matches)] * n if np.isscalar(max_matches) else [int(m) for m in max_matches]
+        bufs = [np.frombuffer(p, np.uint8) for p in pats]
+        outs = [np.zeros(max(m, 1), np.uint32) for m in maxes]
+        P = (ctypes.c_void_p * n)(*[b.ctypes.data for b in bufs])
+        lens = np.array([len(p) for p in pats], np.uint32)
+        mx = np.array(maxes, np.uint32)
+        tot = np.zeros(n, np.uint32)
+        O = (ctypes.c_void_p * n)(*[o.ctypes.data for o in outs])
+        check(_lib.load().ol_search_multi(self._ctx, doc.handle, P, lens.ctypes.data, n, mx.ctypes.data,
+                                          tot.ctypes.data, O), self._ctx)
+        return [SearchResult(int(t), o[: min(int(t), m)].copy()) for t, o, m in zip(tot, outs, maxes)]
 
     def search_raw(self, text, pattern: bytes, max_matches: int, *,
                    max_pattern_len: int | None = MAX_PATTERN_LEN) -> SearchResult:

@@ -118,3 +118,20 @@ def test_streaming_upload_places_every_chunk(parser):
         assert parser.search_document(doc, b"Z", 4).offsets.tolist() == [ln - 1]
         if ln > 1:
             assert parser.search_document(doc, b"A", 4).offsets.tolist() == [0]
+
+
+def test_multi_pattern_passes_match_single_searches(parser):
+    """Up to eight patterns share a pass over the text; each result equals the oracle's."""
+    text = datagen.corpus(6 << 20, 7).tobytes()
+    arr = np.frombuffer(text, np.uint8)
+    pats = datagen.patterns_eight(arr, 7) + [b"|", b"||||", b"- ", b"zzzz-absent", text[100:101], text[5:9],
+                                             b"\n", text[16383:16383 + 2000], b"x" * 5000]
+    doc = parser.upload(text)
+    want = [oracle.find_all(text, p) for p in pats]
+    res = parser.search_document_multi(doc, pats, [max(len(w), 1) for w in want])
+    for p, w, r in zip(pats, want, res):
+        assert r.total_matches == len(w) and np.array_equal(r.offsets, w), p[:16]
+    # truncation per pattern keeps the lowest offsets and the true totals
+    res = parser.search_document_multi(doc, pats[:8], 3)
+    for w, r in zip(want[:8], res):
+        assert r.total_matches == len(w) and np.array_equal(r.offsets, w[:3])
