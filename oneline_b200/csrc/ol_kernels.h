@@ -38,11 +38,13 @@ struct TreeArgs {
     const uint8_t *depth8;
     uint32_t L;
     uint32_t n_tiles;        // ceil(L / kTreeTile)
-    uint64_t *status_fwd;    // n_tiles * kTreeLevels words, zeroed
-    uint64_t *status_bwd;    // n_tiles * kTreeLevels words, zeroed
-    DocStats *stats;         // tree tickets zeroed
+    uint32_t levels;         // max content depth + 1 (<= kTreeLevels)
+    uint32_t *tile_last;     // n_tiles * kTreeLevels: last content line + 1 of each depth in the tile (0: none)
+    uint32_t *tile_first;    // n_tiles * kTreeLevels: first content line of each depth in the tile (NONE: none)
+    uint32_t *in_last;       // exclusive prefix max of tile_last over the tiles
+    uint32_t *in_first;      // exclusive suffix min of tile_first over the tiles
+    DocStats *stats;
     uint32_t *parent;
-    uint8_t *pdepth;         // depth of the parent, 0xFF for none
     uint32_t *subtree_end;   // optional
     uint32_t *first_child;
     uint32_t *next_sibling;

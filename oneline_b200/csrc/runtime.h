@@ -76,7 +76,7 @@ struct ol_tree {
     uint32_t line_count = 0;
     uint32_t capacity = 0;
     bool deep = false;
-    ol::DevBuf parent_buf, pdepth_buf, end_buf, fc_buf, ns_buf;
+    ol::DevBuf parent_buf, end_buf, fc_buf, ns_buf;
 };
 
 namespace ol {

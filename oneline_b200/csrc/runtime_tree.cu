@@ -17,12 +17,10 @@ ol_status tree_alloc(ol_ctx *ctx, ol_tree *t, uint32_t L) {
     uint32_t cap = round_lines(std::max<uint32_t>(L, 1));
     if (t->capacity >= cap && t->parent_buf.ptr) return OL_OK;
     t->parent_buf.release(st);
-    t->pdepth_buf.release(st);
     t->end_buf.release(st);
     t->fc_buf.release(st);
     t->ns_buf.release(st);
     cudaError_t e = t->parent_buf.reserve((size_t)cap * 4, st);
-    if (e == cudaSuccess) e = t->pdepth_buf.reserve(cap, st);
     if (e == cudaSuccess) e = t->end_buf.reserve((size_t)cap * 4, st);
     if (e == cudaSuccess) e = t->fc_buf.reserve((size_t)cap * 4, st);
     if (e == cudaSuccess) e = t->ns_buf.reserve((size_t)cap * 4, st);
@@ -36,25 +34,22 @@ cudaError_t enqueue_tree_fast(ol_ctx *ctx, const ol_doc *d, ol_tree *t) {
     cudaStream_t st = ctx->stream;
     uint32_t L = d->line_count;
     uint32_t n_tiles = (L + kTreeTile - 1) / kTreeTile;
-    size_t words = (size_t)n_tiles * kTreeLevels * 8;
-    cudaError_t e = ctx->scratch_a.reserve(words, st);
-    if (e == cudaSuccess) e = ctx->scratch_b.reserve(words, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->scratch_a.ptr, 0, words, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->scratch_b.ptr, 0, words, st);
-    // zero the tree tickets and the error word of the document's stats
-    if (e == cudaSuccess) e = cudaMemsetAsync(&d->stats->tree_ticket_fwd, 0, 8, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(&d->stats->error, 0, 4, st);
+    size_t words = (size_t)n_tiles * kTreeLevels;
+    cudaError_t e = ctx->scratch_a.reserve(words * 4 * 4, st);
     if (e != cudaSuccess) return e;
     TreeArgs a{};
     a.kinds = d->kinds;
     a.depth8 = d->depth8;
     a.L = L;
     a.n_tiles = n_tiles;
-    a.status_fwd = (uint64_t *)ctx->scratch_a.ptr;
-    a.status_bwd = (uint64_t *)ctx->scratch_b.ptr;
+    a.levels = std::min<uint32_t>(d->max_depth + 1, kTreeLevels);
+    uint32_t *w = (uint32_t *)ctx->scratch_a.ptr;
+    a.tile_last = w;
+    a.tile_first = w + words;
+    a.in_last = w + 2 * words;
+    a.in_first = w + 3 * words;
     a.stats = d->stats;
     a.parent = (uint32_t *)t->parent_buf.ptr;
-    a.pdepth = (uint8_t *)t->pdepth_buf.ptr;
     a.subtree_end = (uint32_t *)t->end_buf.ptr;
     a.first_child = (uint32_t *)t->fc_buf.ptr;
     a.next_sibling = (uint32_t *)t->ns_buf.ptr;
@@ -159,7 +154,6 @@ extern "C" void ol_tree_free(ol_tree *t) {
         std::lock_guard<std::recursive_mutex> g(ctx->mu);
         cudaSetDevice(ctx->device);
         t->parent_buf.release(ctx->stream);
-        t->pdepth_buf.release(ctx->stream);
         t->end_buf.release(ctx->stream);
         t->fc_buf.release(ctx->stream);
         t->ns_buf.release(ctx->stream);

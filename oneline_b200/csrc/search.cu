@@ -36,9 +36,34 @@ struct SearchSmem {
     alignas(16) uint16_t match[kSearchMaxPatterns][SR_THREADS * SR_STEPS];  // per 16-byte piece, position order
 };
 
-// High bit of each byte of x that is zero; may also flag a 0x01 byte right
-// above a zero byte (candidates are verified, so that costs nothing).
-__device__ __forceinline__ uint32_t zero_bytes_loose(uint32_t x) { return (x - 0x01010101u) & ~x & 0x80808080u; }
+// 16 bytes of shared memory starting at any byte offset.
+__device__ __forceinline__ uint4 lds16_unaligned(const uint8_t *smem, uint32_t off) {
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(smem) + (off >> 2);
+    uint32_t sh = (off & 3) * 8;
+    uint32_t a0 = w[0], a1 = w[1], a2 = w[2], a3 = w[3], a4 = w[4];
+    return make_uint4(__funnelshift_r(a0, a1, sh), __funnelshift_r(a1, a2, sh), __funnelshift_r(a2, a3, sh),
+                      __funnelshift_r(a3, a4, sh));
+}
+
+// Bytes [off, off+16) of the text as four words: from shared memory when
+// staged, else from global memory (bytes at or past N read as zero).
+__device__ __forceinline__ uint4 window16(const uint8_t *smem, uint32_t off, bool staged, const uint8_t *g, uint64_t t0,
+                                          uint64_t N) {
+    if (staged) return lds16_unaligned(smem, off);
+    uint8_t b[16];
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+        uint64_t q = t0 + off + r;
+        b[r] = q < N ? __ldg(g + q) : (uint8_t)0;
+    }
+    return *reinterpret_cast<uint4 *>(b);
+}
+
+// 16-bit mask (bit i = byte i) from the high bits of four SWAR words.
+__device__ __forceinline__ uint32_t gather16(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) {
+    auto g = [](uint32_t c) { return (((c >> 7) * 0x00204081u) >> 21) & 0xFu; };
+    return g(c0) | (g(c1) << 4) | (g(c2) << 8) | (g(c3) << 12);
+}
 
 __global__ void __launch_bounds__(SR_THREADS) search_kernel(SearchArgs a) {
     __shared__ SearchSmem sm;
@@ -59,49 +84,47 @@ __global__ void __launch_bounds__(SR_THREADS) search_kernel(SearchArgs a) {
     if (tid == 0) *reinterpret_cast<uint4 *>(&sm.text[kSearchTile + halo]) = make_uint4(0, 0, 0, 0);
     __syncthreads();
 
-    const uint32_t stage_len = kSearchTile + halo;  // tile-local bytes held in shared memory
-    const uint8_t *gtext = a.text;
-
     // Phase A: for each pattern, the 16-bit match mask of each of my pieces.
+    // Filter: first byte (SWAR over the piece) then the last byte (SWAR over the
+    // piece shifted by len-1); verification: every other byte the same way, for
+    // all sixteen starts at once, stopping when no candidate is left.
 #pragma unroll 1
     for (uint32_t p = 0; p < a.np; p++) {
         const uint32_t m = a.pat_len[p];
         const uint8_t *pat = a.pat[p];
-        const uint8_t pf = __ldg(pat), pl = __ldg(pat + m - 1);
-        const uint32_t F4 = pf * 0x01010101u;
+        const uint32_t F4 = __ldg(pat) * 0x01010101u;
         // largest tile-local start whose occurrence ends inside the text
         const int64_t last_ok = (int64_t)N - (int64_t)m - (int64_t)t0;
 #pragma unroll
         for (uint32_t k = 0; k < SR_STEPS; k++) {
             const uint32_t lo = k * 4096 + tid * 16;
-            uint32_t zw[4] = {zero_bytes_loose(v[k].x ^ F4), zero_bytes_loose(v[k].y ^ F4),
-                              zero_bytes_loose(v[k].z ^ F4), zero_bytes_loose(v[k].w ^ F4)};
-            uint32_t mk = 0;
-            if ((zw[0] | zw[1] | zw[2] | zw[3]) && (int64_t)lo <= last_ok) {
+            uint32_t c0 = zero_bytes(v[k].x ^ F4), c1 = zero_bytes(v[k].y ^ F4);
+            uint32_t c2 = zero_bytes(v[k].z ^ F4), c3 = zero_bytes(v[k].w ^ F4);
+            if ((int64_t)lo + 15 > last_ok) {  // starts past last_ok cannot match
+                uint32_t keep[4];
 #pragma unroll
-                for (uint32_t i = 0; i < 4; i++) {
-                    uint32_t zz = zw[i];
-                    while (zz) {
-                        uint32_t b = 4 * i + ((__ffs(zz) - 8) >> 3);
-                        zz &= zz - 1;
-                        uint32_t ls = lo + b;  // tile-local start
-                        if ((int64_t)ls > last_ok) break;
-                        if (sm.text[ls] != pf) continue;  // loose SWAR false positive
-                        bool ok;
-                        if (ls + m <= stage_len) {
-                            ok = sm.text[ls + m - 1] == pl;
-                            for (uint32_t j = 1; ok && j + 1 < m; j++) ok = sm.text[ls + j] == __ldg(pat + j);
-                        } else {
-                            ok = __ldg(gtext + t0 + ls + m - 1) == pl;
-                            for (uint32_t j = 1; ok && j + 1 < m; j++) {
-                                uint32_t q = ls + j;
-                                uint8_t t = q < stage_len ? sm.text[q] : __ldg(gtext + t0 + q);
-                                ok = t == __ldg(pat + j);
-                            }
-                        }
-                        if (ok) mk |= 1u << b;
-                    }
+                for (int i = 0; i < 4; i++) {
+                    int64_t room = last_ok - (int64_t)(lo + 4 * i) + 1;  // valid starts in word i
+                    keep[i] = room <= 0 ? 0u : (room >= 4 ? 0xFFFFFFFFu : ((1u << (8 * room)) - 1u));
                 }
+                c0 &= keep[0];
+                c1 &= keep[1];
+                c2 &= keep[2];
+                c3 &= keep[3];
+            }
+            uint32_t mk = 0;
+            if (c0 | c1 | c2 | c3) {
+                for (uint32_t jj = 1; jj < m; jj++) {
+                    const uint32_t j = jj == 1 ? m - 1 : jj - 1;  // last byte first, then 1, 2, ...
+                    const uint32_t P4 = __ldg(pat + j) * 0x01010101u;
+                    uint4 w = window16(sm.text, lo + j, staged, a.text, t0, N);
+                    c0 &= zero_bytes(w.x ^ P4);
+                    c1 &= zero_bytes(w.y ^ P4);
+                    c2 &= zero_bytes(w.z ^ P4);
+                    c3 &= zero_bytes(w.w ^ P4);
+                    if (!(c0 | c1 | c2 | c3)) break;
+                }
+                mk = gather16(c0, c1, c2, c3);
             }
             sm.match[p][k * SR_THREADS + tid] = (uint16_t)mk;
         }

@@ -9,19 +9,20 @@
 // crates/oneline-simd/src/links.rs:135-180; first_child / next_sibling are
 // derived from those links.
 //
-// Fast path (every content line has depth < 32): two single-pass kernels with
-// a per-level decoupled look-back.
-//   forward : each thread owns 16 consecutive lines; per level k it records the
-//             last line of depth k in its run; a per-level max-scan over the
-//             threads and a per-level look-back over tiles give every thread the
-//             last line of each depth before its run, from which it rebuilds the
-//             ancestor stack as a 32-bit level mask and resolves parents in O(1)
-//             per line. It also stores each line's parent depth (1 byte).
-//   backward: the mirror image (tiles taken from the end, per-level min of the
-//             first line of each depth after a run) gives subtree_end, the next
-//             content line (first_child) and, with the parent depth from the
-//             forward pass, next_sibling: j = subtree_end[i] shares i's parent
-//             exactly when i has no parent or its parent is shallower than j.
+// Fast path (every content line has depth < 32; D = max depth + 1 levels),
+// three kernels over tiles of 4096 lines (256 threads x 16 consecutive lines):
+//   summary : per tile and level k, the last and the first line of depth k;
+//   scan    : per level, the exclusive prefix max (last line before the tile)
+//             and suffix min (first line after it) over the tiles;
+//   resolve : per level, the same scans over the threads of the tile give
+//             every thread the last line of each depth before its run and the
+//             first line of each depth after it. From these it rebuilds the
+//             ancestor stack as a 32-bit level mask and walks its 16 lines
+//             forward (parent in O(1) per line, the parent's depth kept in
+//             registers), then the stack of following lines and walks backward
+//             (subtree_end, next content line = first_child candidate, and
+//             next_sibling: j = subtree_end[i] shares i's parent exactly when i
+//             has no parent or its parent is shallower than j).
 // Replaces crates/oneline-gpu/src/tree.wgsl:128-375 (seven passes).
 //
 // Any-depth path: 32-ary min tree over the depths; each line searches left
@@ -37,247 +38,306 @@ constexpr uint32_t TR_THREADS = 256;
 constexpr uint32_t TR_RUN = 16;
 static_assert(TR_THREADS * TR_RUN == kTreeTile, "tree tile");
 
-struct TreeSmem {
-    uint32_t lvl[kTreeLevels][TR_THREADS];  // run summary, then exclusive scan, then the stack
-    uint32_t in[kTreeLevels];               // look-back result per level
-    uint32_t agg[kTreeLevels];
-    uint32_t tile;
-};
-
 __device__ __forceinline__ uint32_t mask_below(uint32_t d) { return d >= 32 ? 0xFFFFFFFFu : ((1u << d) - 1u); }
 __device__ __forceinline__ uint32_t mask_le(uint32_t d) { return d >= 31 ? 0xFFFFFFFFu : ((2u << d) - 1u); }
 
-__device__ __forceinline__ void load16(const uint8_t *p, uint64_t first, uint32_t L, uint8_t out[16]) {
-    if (first + 16 <= L) {
-        uint4 v = *reinterpret_cast<const uint4 *>(p + first);
-        const uint8_t *b = reinterpret_cast<const uint8_t *>(&v);
-#pragma unroll
-        for (int r = 0; r < 16; r++) out[r] = b[r];
+// The 16 lines of thread `tid` of tile `tile`: kinds and depths packed four per word.
+struct Run {
+    uint4 kd, dp;
+    uint64_t first;
+};
+
+__device__ __forceinline__ Run load_run(const TreeArgs &a, uint32_t tile, uint32_t tid) {
+    Run r;
+    r.first = (uint64_t)tile * kTreeTile + tid * TR_RUN;
+    if (r.first + 16 <= a.L) {
+        r.kd = *reinterpret_cast<const uint4 *>(a.kinds + r.first);
+        r.dp = *reinterpret_cast<const uint4 *>(a.depth8 + r.first);
     } else {
+        uint8_t k[16], d[16];
 #pragma unroll
-        for (int r = 0; r < 16; r++) out[r] = first + r < L ? p[first + r] : 0;
+        for (int i = 0; i < 16; i++) {
+            bool in = r.first + i < a.L;
+            k[i] = in ? a.kinds[r.first + i] : (uint8_t)KIND_BLANK;  // past the end: blank
+            d[i] = in ? a.depth8[r.first + i] : (uint8_t)0;
+        }
+        r.kd = *reinterpret_cast<uint4 *>(k);
+        r.dp = *reinterpret_cast<uint4 *>(d);
+    }
+    return r;
+}
+
+__device__ __forceinline__ uint32_t byte_of(const uint4 &v, int i) {
+    uint32_t w = i < 4 ? v.x : i < 8 ? v.y : i < 12 ? v.z : v.w;
+    return (w >> (8 * (i & 3))) & 0xFF;
+}
+
+// Level of a line for the tree, or 0xFF for a blank line. Depths >= levels
+// cannot reach this path (the host picks the any-depth path for them).
+__device__ __forceinline__ uint32_t level_of(const Run &r, int i, uint32_t levels) {
+    if (byte_of(r.kd, i) == KIND_BLANK) return 0xFF;
+    return min(byte_of(r.dp, i), levels - 1);
+}
+
+// Dynamic shared memory of the summary and resolve kernels: D levels x 256
+// threads of "last line + 1" (forward) followed by the same of "first line"
+// (backward).
+struct TreeSmem {
+    uint32_t *fa, *fb;
+    uint32_t D;
+    __device__ uint32_t &a(uint32_t k, uint32_t t) { return fa[k * TR_THREADS + t]; }
+    __device__ uint32_t &b(uint32_t k, uint32_t t) { return fb[k * TR_THREADS + t]; }
+};
+extern __shared__ uint32_t tree_dyn_smem[];
+
+__device__ __forceinline__ TreeSmem tree_smem(uint32_t D) {
+    TreeSmem s;
+    s.fa = tree_dyn_smem;
+    s.fb = tree_dyn_smem + D * TR_THREADS;
+    s.D = D;
+    return s;
+}
+
+// Pass 1: per tile and level, the last line (+1) and the first line of that depth.
+__global__ void __launch_bounds__(TR_THREADS) tree_summary_kernel(TreeArgs a) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, tile = blockIdx.x;
+    const uint32_t D = a.levels;
+    TreeSmem sm = tree_smem(D);
+    Run r = load_run(a, tile, tid);
+    for (uint32_t k = 0; k < D; k++) {
+        sm.a(k, tid) = 0;
+        sm.b(k, tid) = NONE;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        uint32_t d = level_of(r, i, D);
+        if (d != 0xFF) sm.a(d, tid) = (uint32_t)(r.first + i + 1);
+    }
+#pragma unroll
+    for (int i = 15; i >= 0; i--) {
+        uint32_t d = level_of(r, i, D);
+        if (d != 0xFF) sm.b(d, tid) = (uint32_t)(r.first + i);
+    }
+    __syncthreads();
+    for (uint32_t k = warp; k < D; k += 8) {
+        uint32_t mx = 0, mn = NONE;
+#pragma unroll
+        for (int j = 0; j < TR_THREADS / 32; j++) {
+            mx = max(mx, sm.a(k, j * 32 + lane));
+            mn = min(mn, sm.b(k, j * 32 + lane));
+        }
+        mx = __reduce_max_sync(0xFFFFFFFFu, mx);
+        mn = __reduce_min_sync(0xFFFFFFFFu, mn);
+        if (lane == 0) {
+            a.tile_last[(size_t)tile * kTreeLevels + k] = mx;
+            a.tile_first[(size_t)tile * kTreeLevels + k] = mn;
+        }
     }
 }
 
-__device__ __forceinline__ void store16_u32(uint32_t *p, uint64_t first, uint32_t L, const uint32_t v[16]) {
-    if (first + 16 <= L) {
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-            *reinterpret_cast<uint4 *>(p + first + 4 * q) = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-    } else {
-#pragma unroll
-        for (int r = 0; r < 16; r++)
-            if (first + r < L) p[first + r] = v[r];
+// Pass 2: for each level (one block per level), exclusive prefix max of
+// tile_last and exclusive suffix min of tile_first over the tiles.
+__global__ void __launch_bounds__(1024) tree_scan_kernel(TreeArgs a) {
+    __shared__ uint32_t s_max[32], s_min[32];
+    const uint32_t k = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t T = a.n_tiles;
+    const uint32_t per = (T + 1023) / 1024;
+    const uint32_t lo = min(T, tid * per), hi = min(T, lo + per);
+    uint32_t mx = 0, mn = NONE;
+    for (uint32_t t = lo; t < hi; t++) {
+        mx = max(mx, a.tile_last[(size_t)t * kTreeLevels + k]);
+        mn = min(mn, a.tile_first[(size_t)t * kTreeLevels + k]);
     }
-}
-
-// Warp inclusive scan with max (forward) or min (backward).
-template <bool MAX>
-__device__ __forceinline__ uint32_t warp_scan(uint32_t x, uint32_t lane, bool reverse) {
+    // inclusive scans over threads: max forward, min backward
+    uint32_t imx = mx, imn = mn;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = reverse ? __shfl_down_sync(0xFFFFFFFFu, x, o) : __shfl_up_sync(0xFFFFFFFFu, x, o);
-        bool ok = reverse ? (lane + o < 32) : ((int)lane >= o);
-        if (ok) x = MAX ? max(x, t) : min(x, t);
+        uint32_t t1 = __shfl_up_sync(0xFFFFFFFFu, imx, o);
+        uint32_t t2 = __shfl_down_sync(0xFFFFFFFFu, imn, o);
+        if ((int)lane >= o) imx = max(imx, t1);
+        if (lane + o < 32) imn = min(imn, t2);
     }
-    return x;
+    if (lane == 31) s_max[warp] = imx;
+    if (lane == 0) s_min[warp] = imn;
+    __syncthreads();
+    uint32_t before = 0, after = NONE;  // warps before / after mine
+    for (uint32_t w = 0; w < warp; w++) before = max(before, s_max[w]);
+    for (uint32_t w = warp + 1; w < 32; w++) after = min(after, s_min[w]);
+    uint32_t ex_mx = max(before, lane == 0 ? 0u : __shfl_up_sync(0xFFFFFFFFu, imx, 1));
+    uint32_t ex_mn = min(after, lane == 31 ? NONE : __shfl_down_sync(0xFFFFFFFFu, imn, 1));
+    // walk my tiles: forward exclusive max, then backward exclusive min
+    uint32_t run = ex_mx;
+    for (uint32_t t = lo; t < hi; t++) {
+        a.in_last[(size_t)t * kTreeLevels + k] = run;
+        run = max(run, a.tile_last[(size_t)t * kTreeLevels + k]);
+    }
+    run = ex_mn;
+    for (uint32_t t = hi; t-- > lo;) {
+        a.in_first[(size_t)t * kTreeLevels + k] = run;
+        run = min(run, a.tile_first[(size_t)t * kTreeLevels + k]);
+    }
 }
 
-__global__ void __launch_bounds__(TR_THREADS) tree_forward_kernel(TreeArgs a) {
-    __shared__ TreeSmem sm;
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) sm.tile = atomicAdd(&a.stats->tree_ticket_fwd, 1u);
-    __syncthreads();
-    const uint32_t tile = sm.tile;
-    const uint64_t first = (uint64_t)tile * kTreeTile + tid * TR_RUN;
-
-    uint8_t kd[16], dp[16];
-    load16(a.kinds, first, a.L, kd);
-    load16(a.depth8, first, a.L, dp);
-
-    // Run summary: last line (+1) of each depth in my run; 0 = none.
+// Pass 3: every thread rebuilds the ancestor stack before its 16 lines and
+// the stack of the lines after them, walks forward for parent (and the
+// parent's depth, kept in registers) and backward for subtree_end,
+// first_child and next_sibling.
+__global__ void __launch_bounds__(TR_THREADS) tree_resolve_kernel(TreeArgs a) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, tile = blockIdx.x;
+    const uint32_t D = a.levels;
+    TreeSmem sm = tree_smem(D);
+    Run r = load_run(a, tile, tid);
+    for (uint32_t k = 0; k < D; k++) {
+        sm.a(k, tid) = 0;
+        sm.b(k, tid) = NONE;
+    }
 #pragma unroll
-    for (uint32_t k = 0; k < kTreeLevels; k++) sm.lvl[k][tid] = 0;
+    for (int i = 0; i < 16; i++) {
+        uint32_t d = level_of(r, i, D);
+        if (d != 0xFF) sm.a(d, tid) = (uint32_t)(r.first + i + 1);
+    }
 #pragma unroll
-    for (int r = 0; r < 16; r++)
-        if (first + r < a.L && kd[r] != KIND_BLANK) sm.lvl[min((uint32_t)dp[r], kTreeLevels - 1)][tid] = (uint32_t)(first + r + 1);
+    for (int i = 15; i >= 0; i--) {
+        uint32_t d = level_of(r, i, D);
+        if (d != 0xFF) sm.b(d, tid) = (uint32_t)(r.first + i);
+    }
     __syncthreads();
-
-    // Exclusive max-scan across the threads, per level; warp w owns levels w, w+8, ...
-    for (uint32_t k = warp; k < kTreeLevels; k += 8) {
-        uint32_t run = 0;
+    // Per level: exclusive max over the threads before mine (seeded with the
+    // tiles before this one) and exclusive min over the threads after mine
+    // (seeded with the tiles after this one).
+    for (uint32_t k = warp; k < D; k += 8) {
+        uint32_t run = a.in_last[(size_t)tile * kTreeLevels + k];
         for (uint32_t j = 0; j < TR_THREADS / 32; j++) {
-            uint32_t x = sm.lvl[k][j * 32 + lane];
-            uint32_t inc = warp_scan<true>(x, lane, false);
+            uint32_t x = sm.a(k, j * 32 + lane), inc = x;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+                if ((int)lane >= o) inc = max(inc, t);
+            }
             uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
-            sm.lvl[k][j * 32 + lane] = max(run, lane == 0 ? 0u : prev);
+            sm.a(k, j * 32 + lane) = max(run, lane == 0 ? 0u : prev);
             run = max(run, __shfl_sync(0xFFFFFFFFu, inc, 31));
         }
-        if (lane == 0) sm.agg[k] = run;
-    }
-    __syncthreads();
-
-    // Per-level look-back (lane k carries level k).
-    if (warp == 0) {
-        uint64_t *st = a.status_fwd + (uint64_t)tile * kTreeLevels;
-        uint32_t agg = sm.agg[lane];
-        st_relaxed_u64(st + lane, (uint64_t)agg | (tile == 0 ? LB_PREFIX : LB_AGGREGATE));
-        uint32_t in = 0;
-        if (tile > 0)
-            in = lb_lane_exclusive(a.status_fwd, tile, kTreeLevels, 0u, &a.stats->error,
-                                   [](uint32_t v, uint32_t acc) { return max(v, acc); });
-        if (tile > 0) st_relaxed_u64(st + lane, (uint64_t)max(in, agg) | LB_PREFIX);
-        sm.in[lane] = in;
-    }
-    __syncthreads();
-
-    // Rebuild the ancestor stack before my run: level k is on it iff the last
-    // line of depth k comes after every line of smaller depth.
-    uint32_t M = 0, runmax = 0;
+        run = a.in_first[(size_t)tile * kTreeLevels + k];
+        for (int j = TR_THREADS / 32 - 1; j >= 0; j--) {
+            uint32_t x = sm.b(k, j * 32 + lane), inc = x;
 #pragma unroll
-    for (uint32_t k = 0; k < kTreeLevels; k++) {
-        uint32_t v = max(sm.in[k], sm.lvl[k][tid]);
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t t = __shfl_down_sync(0xFFFFFFFFu, inc, o);
+                if (lane + o < 32) inc = min(inc, t);
+            }
+            uint32_t next = __shfl_down_sync(0xFFFFFFFFu, inc, 1);
+            sm.b(k, j * 32 + lane) = min(run, lane == 31 ? NONE : next);
+            run = min(run, __shfl_sync(0xFFFFFFFFu, inc, 0));
+        }
+    }
+    __syncthreads();
+
+    // Forward: level k is on the ancestor stack iff its last line comes after
+    // every line of smaller depth.
+    uint32_t M = 0, runmax = 0;
+    for (uint32_t k = 0; k < D; k++) {
+        uint32_t v = sm.a(k, tid);
         if (v > runmax) {
             M |= 1u << k;
             runmax = v;
         }
-        sm.lvl[k][tid] = v;  // my column now holds the stack entries (line + 1)
     }
-
-    uint32_t par[16];
-    uint8_t pd[16];
+    uint32_t pdw[4] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};  // parent depth bytes, 0xFF = none
+    uint32_t par[4];
 #pragma unroll
-    for (int r = 0; r < 16; r++) {
-        uint64_t i = first + r;
-        par[r] = NONE;
-        pd[r] = 0xFF;
-        if (i >= a.L || kd[r] == KIND_BLANK) continue;
-        uint32_t d = dp[r];
-        if (d >= kTreeLevels) {
-            atomicOr(&a.stats->error, OL_DEVERR_DEEP);
-            d = kTreeLevels - 1;
+    for (int i = 0; i < 16; i++) {
+        uint32_t d = level_of(r, i, D);
+        uint32_t pv = NONE;
+        if (d != 0xFF) {
+            uint32_t low = M & mask_below(d);
+            if (low) {
+                uint32_t top = 31 - __clz(low);
+                pv = sm.a(top, tid) - 1;
+                pdw[i >> 2] = (pdw[i >> 2] & ~(0xFFu << (8 * (i & 3)))) | (top << (8 * (i & 3)));
+            }
+            M = low | (1u << d);
+            sm.a(d, tid) = (uint32_t)(r.first + i + 1);
         }
-        uint32_t low = M & mask_below(d);
-        if (low) {
-            uint32_t top = 31 - __clz(low);
-            par[r] = sm.lvl[top][tid] - 1;
-            pd[r] = (uint8_t)top;
+        par[i & 3] = pv;
+        if ((i & 3) == 3) {
+            uint64_t at = r.first + (i - 3);
+            if (at + 4 <= a.L) *reinterpret_cast<uint4 *>(a.parent + at) = make_uint4(par[0], par[1], par[2], par[3]);
+            else
+                for (int q = 0; q < 4; q++)
+                    if (at + q < a.L) a.parent[at + q] = par[q];
         }
-        M = low | (1u << d);
-        sm.lvl[d][tid] = (uint32_t)(i + 1);
     }
-    store16_u32(a.parent, first, a.L, par);
-    if (first + 16 <= a.L) {
-        uint4 v;
-        uint8_t *b = reinterpret_cast<uint8_t *>(&v);
-#pragma unroll
-        for (int r = 0; r < 16; r++) b[r] = pd[r];
-        *reinterpret_cast<uint4 *>(a.pdepth + first) = v;
-    } else {
-#pragma unroll
-        for (int r = 0; r < 16; r++)
-            if (first + r < a.L) a.pdepth[first + r] = pd[r];
-    }
-}
 
-__global__ void __launch_bounds__(TR_THREADS) tree_backward_kernel(TreeArgs a) {
-    __shared__ TreeSmem sm;
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) sm.tile = atomicAdd(&a.stats->tree_ticket_bwd, 1u);
-    __syncthreads();
-    const uint32_t order = sm.tile;             // processing order: from the end
-    const uint32_t tile = a.n_tiles - 1 - order;  // line range of this block
-    const uint64_t first = (uint64_t)tile * kTreeTile + tid * TR_RUN;
-
-    uint8_t kd[16], dp[16], pd[16];
-    load16(a.kinds, first, a.L, kd);
-    load16(a.depth8, first, a.L, dp);
-    load16(a.pdepth, first, a.L, pd);
-
-    // Run summary: first line of each depth in my run; NONE = none.
-#pragma unroll
-    for (uint32_t k = 0; k < kTreeLevels; k++) sm.lvl[k][tid] = NONE;
-#pragma unroll
-    for (int r = 15; r >= 0; r--)
-        if (first + r < a.L && kd[r] != KIND_BLANK) sm.lvl[min((uint32_t)dp[r], kTreeLevels - 1)][tid] = (uint32_t)(first + r);
-    __syncthreads();
-
-    // Exclusive suffix min-scan across the threads, per level.
-    for (uint32_t k = warp; k < kTreeLevels; k += 8) {
-        uint32_t run = NONE;
-        for (int j = TR_THREADS / 32 - 1; j >= 0; j--) {
-            uint32_t x = sm.lvl[k][j * 32 + lane];
-            uint32_t inc = warp_scan<false>(x, lane, true);
-            uint32_t next = __shfl_down_sync(0xFFFFFFFFu, inc, 1);
-            sm.lvl[k][j * 32 + lane] = min(run, lane == 31 ? NONE : next);
-            run = min(run, __shfl_sync(0xFFFFFFFFu, inc, 0));
-        }
-        if (lane == 0) sm.agg[k] = run;
-    }
-    __syncthreads();
-
-    if (warp == 0) {
-        uint64_t *st = a.status_bwd + (uint64_t)order * kTreeLevels;
-        uint32_t agg = sm.agg[lane];
-        st_relaxed_u64(st + lane, (uint64_t)agg | (order == 0 ? LB_PREFIX : LB_AGGREGATE));
-        uint32_t in = NONE;
-        if (order > 0)
-            in = lb_lane_exclusive(a.status_bwd, order, kTreeLevels, NONE, &a.stats->error,
-                                   [](uint32_t v, uint32_t acc) { return min(v, acc); });
-        if (order > 0) st_relaxed_u64(st + lane, (uint64_t)min(in, agg) | LB_PREFIX);
-        sm.in[lane] = in;
-    }
-    __syncthreads();
-
-    // Stack of the lines after my run: level k is on it iff the first line of
-    // depth k comes before every line of smaller depth.
-    uint32_t M = 0, runmin = NONE;
-#pragma unroll
-    for (uint32_t k = 0; k < kTreeLevels; k++) {
-        uint32_t v = min(sm.in[k], sm.lvl[k][tid]);
+    // Backward: level k is on the stack of following lines iff its first line
+    // comes before every line of smaller depth; the highest level on it is the
+    // next content line.
+    M = 0;
+    uint32_t runmin = NONE;
+    for (uint32_t k = 0; k < D; k++) {
+        uint32_t v = sm.b(k, tid);
         if (v < runmin) {
             M |= 1u << k;
             runmin = v;
         }
-        sm.lvl[k][tid] = v;
     }
-
-    uint32_t se[16], fc[16], ns[16];
+    uint32_t se[4], fc[4], ns[4];
 #pragma unroll
-    for (int r = 15; r >= 0; r--) {
-        uint64_t i = first + r;
-        se[r] = (uint32_t)(i + 1);
-        fc[r] = NONE;
-        ns[r] = NONE;
-        if (i >= a.L || kd[r] == KIND_BLANK) continue;
-        uint32_t d = min((uint32_t)dp[r], kTreeLevels - 1);
-        if (M) {
-            uint32_t nb = 31 - __clz(M);  // nearest following content line
-            if (nb > d) fc[r] = sm.lvl[nb][tid];
+    for (int i = 15; i >= 0; i--) {
+        uint64_t line = r.first + i;
+        uint32_t d = level_of(r, i, D);
+        uint32_t vse = (uint32_t)(line + 1), vfc = NONE, vns = NONE;
+        if (d != 0xFF) {
+            if (M) {
+                uint32_t nb = 31 - __clz(M);
+                if (nb > d) vfc = sm.b(nb, tid);
+            }
+            uint32_t le = M & mask_le(d);
+            if (le) {
+                uint32_t top = 31 - __clz(le);
+                uint32_t j = sm.b(top, tid);
+                vse = j;
+                uint32_t pd = (pdw[i >> 2] >> (8 * (i & 3))) & 0xFF;
+                if (pd == 0xFF || pd < top) vns = j;
+            } else {
+                vse = a.L;
+            }
+            M = (M & mask_below(d)) | (1u << d);
+            sm.b(d, tid) = (uint32_t)line;
         }
-        uint32_t le = M & mask_le(d);
-        if (le) {
-            uint32_t top = 31 - __clz(le);
-            uint32_t j = sm.lvl[top][tid];
-            se[r] = j;
-            if (pd[r] == 0xFF || pd[r] < top) ns[r] = j;
-        } else {
-            se[r] = a.L;
+        se[i & 3] = vse;
+        fc[i & 3] = vfc;
+        ns[i & 3] = vns;
+        if ((i & 3) == 0) {
+            uint64_t at = line;
+            if (at + 4 <= a.L) {
+                if (a.subtree_end) *reinterpret_cast<uint4 *>(a.subtree_end + at) = make_uint4(se[0], se[1], se[2], se[3]);
+                *reinterpret_cast<uint4 *>(a.first_child + at) = make_uint4(fc[0], fc[1], fc[2], fc[3]);
+                *reinterpret_cast<uint4 *>(a.next_sibling + at) = make_uint4(ns[0], ns[1], ns[2], ns[3]);
+            } else {
+                for (int q = 0; q < 4; q++) {
+                    if (at + q >= a.L) continue;
+                    if (a.subtree_end) a.subtree_end[at + q] = se[q];
+                    a.first_child[at + q] = fc[q];
+                    a.next_sibling[at + q] = ns[q];
+                }
+            }
         }
-        M = (M & mask_below(d)) | (1u << d);
-        sm.lvl[d][tid] = (uint32_t)i;
     }
-    if (a.subtree_end) store16_u32(a.subtree_end, first, a.L, se);
-    store16_u32(a.first_child, first, a.L, fc);
-    store16_u32(a.next_sibling, first, a.L, ns);
 }
 
 cudaError_t launch_tree_fast(const TreeArgs &a, cudaStream_t st) {
     if (a.n_tiles == 0) return cudaSuccess;
-    tree_forward_kernel<<<a.n_tiles, TR_THREADS, 0, st>>>(a);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    tree_backward_kernel<<<a.n_tiles, TR_THREADS, 0, st>>>(a);
+    size_t smem = (size_t)a.levels * TR_THREADS * 4 * 2;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(tree_summary_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(tree_resolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    tree_summary_kernel<<<a.n_tiles, TR_THREADS, smem, st>>>(a);
+    tree_scan_kernel<<<a.levels, 1024, 0, st>>>(a);
+    tree_resolve_kernel<<<a.n_tiles, TR_THREADS, smem, st>>>(a);
     return cudaGetLastError();
 }
 
