@@ -163,8 +163,11 @@ __global__ void __launch_bounds__(1024) tree_scan_kernel(TreeArgs a) {
     uint32_t before = 0, after = NONE;  // warps before / after mine
     for (uint32_t w = 0; w < warp; w++) before = max(before, s_max[w]);
     for (uint32_t w = warp + 1; w < 32; w++) after = min(after, s_min[w]);
-    uint32_t ex_mx = max(before, lane == 0 ? 0u : __shfl_up_sync(0xFFFFFFFFu, imx, 1));
-    uint32_t ex_mn = min(after, lane == 31 ? NONE : __shfl_down_sync(0xFFFFFFFFu, imn, 1));
+    // every lane takes part in both shuffles; lanes 0 / 31 discard the result
+    const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, imx, 1);
+    const uint32_t down = __shfl_down_sync(0xFFFFFFFFu, imn, 1);
+    uint32_t ex_mx = max(before, lane == 0 ? 0u : up);
+    uint32_t ex_mn = min(after, lane == 31 ? NONE : down);
     // walk my tiles: forward exclusive max, then backward exclusive min
     uint32_t run = ex_mx;
     for (uint32_t t = lo; t < hi; t++) {
