@@ -282,7 +282,7 @@ def run_ours(args, world, rank, local):
         enqueue_tree()
         enqueue_search()
 
-    launches_per_step = 2 + 2 + (n_p + 7) // 8
+    launches_per_step = 2 + 3 + (n_p + 7) // 8  # parse (tiles, fix-up), tree (summary, scan, resolve), search
     if args.profile_launches:
         for _ in range(args.warmup + args.steps):
             step()

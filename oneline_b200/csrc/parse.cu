@@ -28,7 +28,6 @@ constexpr uint32_t PT_TILE = PT_THREADS * 16 * PT_STEPS;  // 16384
 constexpr uint32_t PT_HALO = 256;
 constexpr uint32_t PT_LIST = 1024;                        // newline positions listed per round
 constexpr uint32_t PT_WORKERS = PT_THREADS - 32;          // warps 1..7 classify, warp 0 looks back
-constexpr uint32_t PT_PER_WORKER = (PT_LIST + PT_WORKERS - 1) / PT_WORKERS;  // 10
 
 static_assert(PT_TILE == kParseTile && PT_HALO == kParseHalo, "tile geometry");
 
@@ -37,14 +36,16 @@ struct ParseSmem {
     uint16_t nl[PT_LIST + 1];        // newline positions of the current round, ascending
     uint32_t warp_tot[PT_STEPS][8];  // newline count per (step, warp)
     uint32_t warp_base[PT_STEPS][8];
+    uint32_t res_off[PT_LIST];       // per line of the round: its start (tile-local)
+    uint16_t res_pk[PT_LIST];        // kind | min(depth, 255) << 8, or PK_NONE / PK_FIXUP
     uint32_t halo_first;             // first newline in the halo (local), or NONE
     uint32_t nl_base;                // newlines before this tile
     uint32_t n_nl;                   // newlines in this tile
 };
 
-// Packed per-line result kept in registers until the tile's line base is known.
-constexpr uint32_t PK_NONE = 0xFFFFFFFFu;   // no line in this slot
-constexpr uint32_t PK_FIXUP = 0xFFFFFFFEu;  // offset only; the fix-up kernel classifies it
+// Packed per-line result held in shared memory until the tile's line base is known.
+constexpr uint16_t PK_NONE = 0xFFFF;   // no line in this slot
+constexpr uint16_t PK_FIXUP = 0xFFFE;  // offset only; the fix-up kernel classifies it
 
 // 4 bytes of shared memory from any byte offset.
 __device__ __forceinline__ uint32_t lds4(const uint8_t *base, uint32_t off) {
@@ -92,7 +93,7 @@ __device__ __forceinline__ uint32_t classify_smem(const uint8_t *t, uint32_t s, 
     return classify3((uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), n);
 }
 
-__global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a) {
+__global__ void __launch_bounds__(PT_THREADS, 8) parse_tiles_kernel(ParseArgs a) {
     __shared__ ParseSmem sm;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;
@@ -219,7 +220,7 @@ __global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a)
         }
         __syncthreads();  // (c) list ready
 
-        uint32_t res_off[PT_PER_WORKER], res_pk[PT_PER_WORKER];
+        const uint32_t r_end = min(n_lines, r0 + PT_LIST);
         if (warp == 0) {
             if (!base_known) {
                 uint32_t nl_base = tile == 0 ? 0u : lb_sum_exclusive(a.tile_status, tile, &a.stats->error);
@@ -233,54 +234,54 @@ __global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a)
                 }
             }
         } else {
-#pragma unroll
-            for (uint32_t i = 0; i < PT_PER_WORKER; i++) {
-                uint32_t j = r0 + (tid - 32) + i * PT_WORKERS;
-                res_pk[i] = PK_NONE;
-                res_off[i] = 0;
-                if (j >= n_lines || j >= r0 + PT_LIST) continue;
+            for (uint32_t j = r0 + (tid - 32); j < r_end; j += PT_WORKERS) {
                 int32_t q = (int32_t)j - (int32_t)off;  // newline that precedes the line (-1: none)
                 uint32_t s = q < 0 ? 0u : sm.nl[q - w0] + 1u;  // tile-local
-                if (s >= valid) continue;  // the final '\n' starts no line
-                res_off[i] = (uint32_t)t0 + s;
-                uint32_t e;
-                if ((uint32_t)(q + 1) < n_nl) e = sm.nl[q + 1 - w0];
-                else if (halo_first != NONE) e = halo_first;
-                else if (valid < PT_TILE + PT_HALO) e = valid;  // the text ends in the staged bytes
-                else {
-                    res_pk[i] = PK_FIXUP;  // runs past the halo
-                    continue;
+                uint16_t pk = PK_NONE;
+                if (s < valid) {  // the final '\n' starts no line
+                    uint32_t e;
+                    bool known = true;
+                    if ((uint32_t)(q + 1) < n_nl) e = sm.nl[q + 1 - w0];
+                    else if (halo_first != NONE) e = halo_first;
+                    else if (valid < PT_TILE + PT_HALO) e = valid;  // the text ends in the staged bytes
+                    else known = false;                            // runs past the halo
+                    if (known) {
+                        uint32_t depth, cs, eff;
+                        uint32_t kind = classify_smem(sm.text, s, e, depth, cs, eff);
+                        pk = (uint16_t)(kind | (min(depth, 255u) << 8));
+                        if (kind != KIND_BLANK) my_max = max(my_max, depth);
+                    } else {
+                        pk = PK_FIXUP;
+                    }
                 }
-                uint32_t depth, cs, eff;
-                uint32_t kind = classify_smem(sm.text, s, e, depth, cs, eff);
-                res_pk[i] = kind | (min(depth, 255u) << 8);
-                if (kind != KIND_BLANK) my_max = max(my_max, depth);
+                sm.res_off[j - r0] = s;
+                sm.res_pk[j - r0] = pk;
             }
         }
-        __syncthreads();  // (d) base known; the list may be rewritten
+        __syncthreads();  // (d) base and results known
         base_known = true;
         const uint32_t nl_base = sm.nl_base;
-        if (warp != 0) {
-#pragma unroll
-            for (uint32_t i = 0; i < PT_PER_WORKER; i++) {
-                if (res_pk[i] == PK_NONE) continue;
-                uint32_t j = r0 + (tid - 32) + i * PT_WORKERS;
-                uint32_t idx = nl_base + j + 1 - off;
-                if (idx >= a.line_cap) {
-                    atomicOr(&a.stats->error, OL_DEVERR_CAPACITY);
-                    continue;
-                }
-                a.offsets[idx] = res_off[i];
-                if (res_pk[i] == PK_FIXUP) {
-                    uint32_t slot = atomicAdd(&a.stats->fixup_count, 1u);
-                    if (slot < a.fixup_cap) a.fixup[slot] = make_uint2(idx, res_off[i]);
-                    else atomicOr(&a.stats->error, OL_DEVERR_FIXUP);
-                    continue;
-                }
-                a.kinds[idx] = (uint8_t)(res_pk[i] & 0xFF);
-                a.depth8[idx] = (uint8_t)(res_pk[i] >> 8);
+        // All threads write the round's lines in order: coalesced.
+        for (uint32_t j = r0 + tid; j < r_end; j += PT_THREADS) {
+            uint16_t pk = sm.res_pk[j - r0];
+            if (pk == PK_NONE) continue;
+            uint32_t idx = nl_base + j + 1 - off;
+            uint32_t start = (uint32_t)t0 + sm.res_off[j - r0];
+            if (idx >= a.line_cap) {
+                atomicOr(&a.stats->error, OL_DEVERR_CAPACITY);
+                continue;
             }
+            a.offsets[idx] = start;
+            if (pk == PK_FIXUP) {
+                uint32_t slot = atomicAdd(&a.stats->fixup_count, 1u);
+                if (slot < a.fixup_cap) a.fixup[slot] = make_uint2(idx, start);
+                else atomicOr(&a.stats->error, OL_DEVERR_FIXUP);
+                continue;
+            }
+            a.kinds[idx] = (uint8_t)(pk & 0xFF);
+            a.depth8[idx] = (uint8_t)(pk >> 8);
         }
+        __syncthreads();  // (e) the next round may overwrite the list and results
     }
     for (int o = 16; o > 0; o >>= 1) my_max = max(my_max, __shfl_xor_sync(0xFFFFFFFFu, my_max, o));
     if (lane == 0 && my_max) atomicMax(&a.stats->max_content_depth, my_max);

@@ -45,6 +45,10 @@ __device__ __forceinline__ uint4 lds16_unaligned(const uint8_t *smem, uint32_t o
                       __funnelshift_r(a3, a4, sh));
 }
 
+// High bit of each byte of x that is zero; may also flag a 0x01 byte right
+// above a zero byte (a cheap first filter, confirmed by zero_bytes).
+__device__ __forceinline__ uint32_t zero_bytes_loose(uint32_t x) { return (x - 0x01010101u) & ~x & 0x80808080u; }
+
 // Bytes [off, off+16) of the text as four words: from shared memory when
 // staged, else from global memory (bytes at or past N read as zero).
 __device__ __forceinline__ uint4 window16(const uint8_t *smem, uint32_t off, bool staged, const uint8_t *g, uint64_t t0,
@@ -88,33 +92,40 @@ __global__ void __launch_bounds__(SR_THREADS) search_kernel(SearchArgs a) {
     // Filter: first byte (SWAR over the piece) then the last byte (SWAR over the
     // piece shifted by len-1); verification: every other byte the same way, for
     // all sixteen starts at once, stopping when no candidate is left.
+    // Only the last tiles hold starts whose occurrence would run past the text.
+    const bool tail_tile = t0 + kSearchTile + a.halo + 16 > N;
 #pragma unroll 1
     for (uint32_t p = 0; p < a.np; p++) {
         const uint32_t m = a.pat_len[p];
         const uint8_t *pat = a.pat[p];
         const uint32_t F4 = __ldg(pat) * 0x01010101u;
-        // largest tile-local start whose occurrence ends inside the text
-        const int64_t last_ok = (int64_t)N - (int64_t)m - (int64_t)t0;
 #pragma unroll
         for (uint32_t k = 0; k < SR_STEPS; k++) {
             const uint32_t lo = k * 4096 + tid * 16;
-            uint32_t c0 = zero_bytes(v[k].x ^ F4), c1 = zero_bytes(v[k].y ^ F4);
-            uint32_t c2 = zero_bytes(v[k].z ^ F4), c3 = zero_bytes(v[k].w ^ F4);
-            if ((int64_t)lo + 15 > last_ok) {  // starts past last_ok cannot match
-                uint32_t keep[4];
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    int64_t room = last_ok - (int64_t)(lo + 4 * i) + 1;  // valid starts in word i
-                    keep[i] = room <= 0 ? 0u : (room >= 4 ? 0xFFFFFFFFu : ((1u << (8 * room)) - 1u));
-                }
-                c0 &= keep[0];
-                c1 &= keep[1];
-                c2 &= keep[2];
-                c3 &= keep[3];
-            }
+            // loose first-byte filter: 3 operations per word
+            uint32_t c0 = zero_bytes_loose(v[k].x ^ F4), c1 = zero_bytes_loose(v[k].y ^ F4);
+            uint32_t c2 = zero_bytes_loose(v[k].z ^ F4), c3 = zero_bytes_loose(v[k].w ^ F4);
             uint32_t mk = 0;
             if (c0 | c1 | c2 | c3) {
-                for (uint32_t jj = 1; jj < m; jj++) {
+                // exact first byte (drops the loose test's false positives)
+                c0 = zero_bytes(v[k].x ^ F4);
+                c1 = zero_bytes(v[k].y ^ F4);
+                c2 = zero_bytes(v[k].z ^ F4);
+                c3 = zero_bytes(v[k].w ^ F4);
+                if (tail_tile) {  // starts past N - m cannot match
+                    const int64_t last_ok = (int64_t)N - (int64_t)m - (int64_t)t0;
+                    uint32_t keep[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        int64_t room = last_ok - (int64_t)(lo + 4 * i) + 1;  // valid starts in word i
+                        keep[i] = room <= 0 ? 0u : (room >= 4 ? 0xFFFFFFFFu : ((1u << (8 * room)) - 1u));
+                    }
+                    c0 &= keep[0];
+                    c1 &= keep[1];
+                    c2 &= keep[2];
+                    c3 &= keep[3];
+                }
+                for (uint32_t jj = 1; jj < m && (c0 | c1 | c2 | c3); jj++) {
                     const uint32_t j = jj == 1 ? m - 1 : jj - 1;  // last byte first, then 1, 2, ...
                     const uint32_t P4 = __ldg(pat + j) * 0x01010101u;
                     uint4 w = window16(sm.text, lo + j, staged, a.text, t0, N);
@@ -122,7 +133,6 @@ __global__ void __launch_bounds__(SR_THREADS) search_kernel(SearchArgs a) {
                     c1 &= zero_bytes(w.y ^ P4);
                     c2 &= zero_bytes(w.z ^ P4);
                     c3 &= zero_bytes(w.w ^ P4);
-                    if (!(c0 | c1 | c2 | c3)) break;
                 }
                 mk = gather16(c0, c1, c2, c3);
             }
