@@ -137,6 +137,56 @@ __device__ __forceinline__ uint32_t lb_sum_exclusive(const uint64_t *status, uin
     return acc;
 }
 
+// The same over 128-tile windows: lane l covers tiles [end-128+4l, +4). One
+// window costs one round trip to L2, so the walk keeps up with tiles that
+// finish faster than 32 per round trip.
+__device__ __forceinline__ uint32_t lb_sum_exclusive_wide(const uint64_t *status, uint32_t tile, uint32_t *err,
+                                                          uint32_t stride = 1) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t acc = 0;
+    int64_t end = (int64_t)tile;  // window is [end-128, end)
+    while (end > 0) {
+        int64_t base = end - 128 + 4 * (int64_t)lane;
+        uint64_t w[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int64_t idx = base + i;
+            w[i] = idx >= 0 ? ld_relaxed_u64(status + idx * stride) : LB_PREFIX;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int64_t idx = base + i;
+            if (!(w[i] & LB_STATUS_MASK)) w[i] = lb_wait(status + idx * stride, err);
+        }
+        // highest tile of mine holding a prefix (-1: none)
+        int hi_mine = -1;
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            if ((w[i] & LB_STATUS_MASK) == LB_PREFIX) hi_mine = i;
+        uint32_t lanes_with_prefix = __ballot_sync(0xFFFFFFFFu, hi_mine >= 0);
+        uint32_t v = 0;
+        if (lanes_with_prefix) {
+            int hl = 31 - __clz(lanes_with_prefix);  // lane holding the nearest prefix
+            if ((int)lane > hl) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) v += (uint32_t)w[i];
+            } else if ((int)lane == hl) {
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+                    if (i >= hi_mine) v += (uint32_t)w[i];
+            }
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+            return acc + v;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) v += (uint32_t)w[i];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        acc += v;
+        end -= 128;
+    }
+    return acc;
+}
+
 // Per-lane look-back for lanes that each carry an independent value chain
 // (one value per tile per lane at status + tile*stride + lane). `op` combines
 // an older tile's value into the running value; walking stops at the first

@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(PT_THREADS, 8) parse_tiles_kernel(ParseArgs a)
         const uint32_t r_end = min(n_lines, r0 + PT_LIST);
         if (warp == 0) {
             if (!base_known) {
-                uint32_t nl_base = tile == 0 ? 0u : lb_sum_exclusive(a.tile_status, tile, &a.stats->error);
+                uint32_t nl_base = tile == 0 ? 0u : lb_sum_exclusive_wide(a.tile_status, tile, &a.stats->error);
                 if (lane == 0) {
                     sm.nl_base = nl_base;
                     if (tile != 0) st_relaxed_u64(a.tile_status + tile, (uint64_t)(nl_base + n_nl) | LB_PREFIX);
