@@ -282,7 +282,8 @@ def run_ours(args, world, rank, local):
         enqueue_tree()
         enqueue_search()
 
-    launches_per_step = 2 + 3 + (n_p + 7) // 8  # parse (tiles, fix-up), tree (summary, scan, resolve), search
+    # parse: count, scan, tiles, fix-up; tree: summary, scan, resolve; search: count, scan, write per 8 patterns
+    launches_per_step = 4 + 3 + 3 * ((n_p + 7) // 8)
     if args.profile_launches:
         for _ in range(args.warmup + args.steps):
             step()

@@ -19,8 +19,9 @@ struct ParseArgs {
     const uint8_t *text;  // padded: n_tiles * kParseTile + kParseHalo readable bytes
     uint64_t text_len;
     uint32_t n_tiles;
-    uint64_t *tile_status;  // n_tiles words, zeroed before the launch
-    DocStats *stats;        // ticket/fixup_count/error zeroed before the launch
+    uint32_t *tile_count;   // n_tiles newline counts (pass 1)
+    uint32_t *tile_base;    // n_tiles exclusive prefix sums (pass 2)
+    DocStats *stats;        // fixup_count/error zeroed before the launch
     uint32_t *offsets;      // line_cap entries
     uint8_t *kinds;
     uint8_t *depth8;        // min(depth, 255)
@@ -30,6 +31,11 @@ struct ParseArgs {
 };
 
 cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st);
+
+// Exclusive scan of the first `cols` columns of a row-major [rows][stride] u32
+// matrix (one block per column); totals[c] (optional) receives column c's sum.
+cudaError_t launch_scan_columns(const uint32_t *in, uint32_t *out, uint32_t *totals, uint32_t rows, uint32_t cols,
+                                uint32_t stride, cudaStream_t st);
 cudaError_t launch_classify_lines(const uint8_t *text, uint64_t N, const uint32_t *offsets, uint32_t L, FlatNode *nodes,
                                   uint32_t *depth32, cudaStream_t st);
 
@@ -81,9 +87,9 @@ struct SearchArgs {
     uint32_t pat_len[kSearchMaxPatterns];
     uint32_t *out[kSearchMaxPatterns];          // ascending offsets, first max_out[p] of them
     uint32_t max_out[kSearchMaxPatterns];
-    uint64_t *tile_status;   // n_tiles * kSearchMaxPatterns words, zeroed
-    uint32_t *totals;        // np totals, written by the last tile
-    uint32_t *error;
+    uint32_t *counts;        // [n_tiles][kSearchMaxPatterns] matches per tile (pass 1)
+    uint32_t *bases;         // [n_tiles][kSearchMaxPatterns] exclusive scans (pass 2)
+    uint32_t *totals;        // kSearchMaxPatterns totals (pass 2)
 };
 
 cudaError_t launch_search(const SearchArgs &a, cudaStream_t st);

@@ -1,15 +1,18 @@
 // Kernel (a)+(b): newline scan fused with per-line classification.
 //
-// One pass over the text. CTA b owns the 16 KiB tile b (blocks are dispatched in
-// index order, so the tiles a block looks back on are already running); it loads
-// the tile with 16-byte coalesced vector loads, finds its newlines with byte
-// SWAR, ranks them in position order with warp popc scans, publishes its newline
-// count at once, and then, while warp 0 runs the single-pass decoupled look-back
-// for the tile's global line base, warps 1..7 classify every line that starts
-// after one of the tile's newlines from shared memory. Results wait in
-// registers and are written, coalesced, once the base is known. A line that
-// runs past the tile plus a 256-byte halo is queued for a small fix-up kernel,
-// which reads it from global memory once the offsets array is complete.
+// Three launches, no block ever waits on another:
+//   1. newline_count_kernel: per 16 KiB tile, the newline count (16-byte
+//      coalesced vector loads, exact byte SWAR, popc, warp reductions);
+//   2. scan_columns_kernel: exclusive scan of the tile counts = every tile's
+//      first line index;
+//   3. parse_tiles_kernel: per tile, the newline positions in order (warp popc
+//      scans) and the classification of every line starting in the tile, from
+//      shared memory, written coalesced at the line indices from step 2.
+// The text is read twice from HBM; a single pass with a decoupled look-back
+// was measured slower here: the look-back chain fell behind the tile rate.
+// A line that runs past the tile plus a 256-byte halo is queued for a small
+// fix-up kernel, which reads it from global memory once the offsets array is
+// complete.
 //
 // Replaces crates/oneline-gpu/src/scan.wgsl:20-237 (three passes + a host read
 // of the line count) and shader.wgsl:34-134 (one thread per line, byte loads
@@ -27,7 +30,6 @@ constexpr uint32_t PT_STEPS = 4;                          // 16-byte pieces per 
 constexpr uint32_t PT_TILE = PT_THREADS * 16 * PT_STEPS;  // 16384
 constexpr uint32_t PT_HALO = 256;
 constexpr uint32_t PT_LIST = 1024;                        // newline positions listed per round
-constexpr uint32_t PT_WORKERS = PT_THREADS - 32;          // warps 1..7 classify, warp 0 looks back
 
 static_assert(PT_TILE == kParseTile && PT_HALO == kParseHalo, "tile geometry");
 
@@ -36,16 +38,8 @@ struct ParseSmem {
     uint16_t nl[PT_LIST + 1];        // newline positions of the current round, ascending
     uint32_t warp_tot[PT_STEPS][8];  // newline count per (step, warp)
     uint32_t warp_base[PT_STEPS][8];
-    uint32_t res_off[PT_LIST];       // per line of the round: its start (tile-local)
-    uint16_t res_pk[PT_LIST];        // kind | min(depth, 255) << 8, or PK_NONE / PK_FIXUP
     uint32_t halo_first;             // first newline in the halo (local), or NONE
-    uint32_t nl_base;                // newlines before this tile
-    uint32_t n_nl;                   // newlines in this tile
 };
-
-// Packed per-line result held in shared memory until the tile's line base is known.
-constexpr uint16_t PK_NONE = 0xFFFF;   // no line in this slot
-constexpr uint16_t PK_FIXUP = 0xFFFE;  // offset only; the fix-up kernel classifies it
 
 // 4 bytes of shared memory from any byte offset.
 __device__ __forceinline__ uint32_t lds4(const uint8_t *base, uint32_t off) {
@@ -62,8 +56,7 @@ __device__ __forceinline__ uint32_t blank_bits(uint32_t w) {
 // parse_line (crates/oneline-simd/src/line.rs:8-44) for a line held in shared
 // memory at tile-local [s, e), e = its '\n' or the text end; the bytes from e
 // to e+3 are readable. Same rules as classify_line, four bytes per step.
-__device__ __forceinline__ uint32_t classify_smem(const uint8_t *t, uint32_t s, uint32_t e, uint32_t &depth_out,
-                                                  uint32_t &cs_out, uint32_t &eff_out) {
+__device__ __forceinline__ uint32_t classify_smem(const uint8_t *t, uint32_t s, uint32_t e, uint32_t &depth_out) {
     uint32_t eff = e;
     while (eff > s && t[eff - 1] == '\r') eff--;
     uint32_t c = s, depth = 0;
@@ -85,14 +78,63 @@ __device__ __forceinline__ uint32_t classify_smem(const uint8_t *t, uint32_t s, 
     // be followed by nothing: clamp to eff
     if (c > eff) c = eff;
     depth_out = depth;
-    cs_out = c;
-    eff_out = eff;
     if (c >= eff) return KIND_BLANK;
-    uint32_t n = eff - c;
     uint32_t w = lds4(t, c);
-    return classify3((uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), n);
+    return classify3((uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), eff - c);
 }
 
+// Exact '\n' bits (high bit of each byte) of a 16-byte piece at tile-local lo;
+// bytes at or past `valid` are cleared.
+__device__ __forceinline__ void newline_bits(const uint4 &v, uint32_t lo, uint32_t valid, uint32_t z[4]) {
+    const uint32_t NL4 = 0x0A0A0A0Au;
+    z[0] = zero_bytes(v.x ^ NL4);
+    z[1] = zero_bytes(v.y ^ NL4);
+    z[2] = zero_bytes(v.z ^ NL4);
+    z[3] = zero_bytes(v.w ^ NL4);
+    if (lo + 16 > valid) {
+#pragma unroll
+        for (uint32_t i = 0; i < 4; i++) {
+            uint32_t b0 = lo + 4 * i;  // bytes b0..b0+3; keep those < valid
+            uint32_t keep = b0 >= valid ? 0u : (valid - b0 >= 4 ? 4u : valid - b0);
+            z[i] &= keep == 4 ? 0xFFFFFFFFu : ((1u << (8 * keep)) - 1u);
+        }
+    }
+}
+
+// Pass 1: newlines per 16 KiB tile (positions < N).
+__global__ void __launch_bounds__(PT_THREADS) newline_count_kernel(const uint8_t *__restrict__ text, uint64_t N,
+                                                                    uint32_t *__restrict__ counts) {
+    __shared__ uint32_t warp_sum[PT_THREADS / 32];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t t0 = (uint64_t)blockIdx.x * PT_TILE;
+    const uint32_t valid = N - t0 >= PT_TILE ? PT_TILE : (uint32_t)(N - t0);
+    uint4 v[PT_STEPS];
+#pragma unroll
+    for (uint32_t k = 0; k < PT_STEPS; k++) v[k] = ld_stream16(text + t0 + k * 4096 + tid * 16);
+    uint32_t c = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < PT_STEPS; k++) {
+        uint32_t z[4];
+        newline_bits(v[k], k * 4096 + tid * 16, valid, z);
+        c += __popc(z[0]) + __popc(z[1]) + __popc(z[2]) + __popc(z[3]);
+    }
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if (lane == 0) warp_sum[warp] = c;
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t t = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < PT_THREADS / 32; w++) t += warp_sum[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// Pass 3: CTA b re-reads tile b, lists its newlines in position order (warp
+// popc scans) and classifies every line that starts after one of them (plus
+// line 0 for tile 0) from shared memory, knowing the tile's first line index
+// from the scan of pass 2. Consecutive threads take consecutive lines, so the
+// outputs are written coalesced. A line that runs past the tile plus a
+// 256-byte halo is queued for the fix-up kernel.
 __global__ void __launch_bounds__(PT_THREADS, 8) parse_tiles_kernel(ParseArgs a) {
     __shared__ ParseSmem sm;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -116,29 +158,15 @@ __global__ void __launch_bounds__(PT_THREADS, 8) parse_tiles_kernel(ParseArgs a)
     for (uint32_t k = 0; k < PT_STEPS; k++) *reinterpret_cast<uint4 *>(&sm.text[k * 4096 + tid * 16]) = v[k];
     if (tid < PT_HALO / 16) *reinterpret_cast<uint4 *>(&sm.text[PT_TILE + tid * 16]) = vh;
 
-    // 2. Newline bits: z[k][i] has the high bit of each '\n' byte of word i of
-    //    piece k (exact SWAR test; bytes at or past the text end cleared).
-    const uint32_t NL4 = 0x0A0A0A0Au;
+    // 2. Newline bits and their ranks within the warp: steps (0,1) and (2,3)
+    //    packed in 16-bit fields.
     uint32_t z[PT_STEPS][4];
     uint32_t cnt[PT_STEPS];
 #pragma unroll
     for (uint32_t k = 0; k < PT_STEPS; k++) {
-        const uint32_t lo = k * 4096 + tid * 16;
-        z[k][0] = zero_bytes(v[k].x ^ NL4);
-        z[k][1] = zero_bytes(v[k].y ^ NL4);
-        z[k][2] = zero_bytes(v[k].z ^ NL4);
-        z[k][3] = zero_bytes(v[k].w ^ NL4);
-        if (lo + 16 > valid) {
-#pragma unroll
-            for (uint32_t i = 0; i < 4; i++) {
-                uint32_t b0 = lo + 4 * i;  // bytes b0..b0+3; keep those < valid
-                uint32_t keep = b0 >= valid ? 0u : (valid - b0 >= 4 ? 4u : valid - b0);
-                z[k][i] &= keep == 4 ? 0xFFFFFFFFu : ((1u << (8 * keep)) - 1u);
-            }
-        }
+        newline_bits(v[k], k * 4096 + tid * 16, valid, z[k]);
         cnt[k] = __popc(z[k][0]) + __popc(z[k][1]) + __popc(z[k][2]) + __popc(z[k][3]);
     }
-    // Ranks within the warp: steps (0,1) and (2,3) packed in 16-bit fields.
     uint32_t c01 = cnt[0] | (cnt[1] << 16), c23 = cnt[2] | (cnt[3] << 16);
     uint32_t i01 = c01, i23 = c23;
 #pragma unroll
@@ -161,15 +189,11 @@ __global__ void __launch_bounds__(PT_THREADS, 8) parse_tiles_kernel(ParseArgs a)
     if (tid < PT_HALO / 16) {
         const uint32_t lo = PT_TILE + tid * 16;
         uint32_t first = NONE;
-        uint32_t hw[4] = {vh.x, vh.y, vh.z, vh.w};
+        uint32_t zh[4];
+        newline_bits(vh, lo, valid, zh);
 #pragma unroll
-        for (int i = 3; i >= 0; i--) {
-            uint32_t zz = zero_bytes(hw[i] ^ NL4);
-            uint32_t b0 = lo + 4 * i;
-            uint32_t keep = b0 >= valid ? 0u : (valid - b0 >= 4 ? 4u : valid - b0);
-            zz &= keep == 4 ? 0xFFFFFFFFu : ((1u << (8 * keep)) - 1u);
-            if (zz) first = b0 + ((__ffs(zz) - 8) >> 3);
-        }
+        for (int i = 3; i >= 0; i--)
+            if (zh[i]) first = lo + 4 * i + ((__ffs(zh[i]) - 8) >> 3);
         for (int o = 8; o > 0; o >>= 1) first = min(first, __shfl_xor_sync(0x0000FFFFu, first, o));
         if (tid == 0) sm.halo_first = first;
     }
@@ -182,25 +206,22 @@ __global__ void __launch_bounds__(PT_THREADS, 8) parse_tiles_kernel(ParseArgs a)
             if ((int)lane >= o) inc += t;
         }
         sm.warp_base[lane >> 3][lane & 7] = inc - c;
-        uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
-        if (lane == 0) {
-            sm.n_nl = total;
-            // Publish the aggregate at once (tile 0 publishes its prefix).
-            st_relaxed_u64(a.tile_status + tile, (uint64_t)total | (tile == 0 ? LB_PREFIX : LB_AGGREGATE));
-        }
     }
-    __syncthreads();  // (b) bases and n_nl visible
+    __syncthreads();  // (b) bases and halo_first visible
 
-    const uint32_t n_nl = sm.n_nl, off = tile == 0 ? 1u : 0u;
+    const uint32_t nl_base = a.tile_base[tile];  // newlines before this tile
+    const uint32_t n_nl = a.tile_count[tile];
+    const uint32_t off = tile == 0 ? 1u : 0u;
     const uint32_t n_lines = n_nl + off;
     const uint32_t halo_first = sm.halo_first;
+    if (tile == a.n_tiles - 1 && tid == 0)  // L = 1 + newlines before the last byte
+        a.stats->line_count = 1u + nl_base + n_nl - (a.text[N - 1] == '\n');
     uint32_t my_max = 0;
-    bool base_known = false;
 
     // Lines are classified in rounds of PT_LIST (one round unless the tile
     // holds more than 1024 newlines): list the round's newline positions, then
-    // warps 1..7 classify while warp 0 runs the look-back (first round only).
-    for (uint32_t r0 = 0; r0 < n_lines || (r0 == 0 && !base_known); r0 += PT_LIST) {
+    // classify and write the round's lines.
+    for (uint32_t r0 = 0; r0 < n_lines; r0 += PT_LIST) {
         const int32_t w0 = (int32_t)r0 - (int32_t)off;  // rank of nl[0]
 #pragma unroll
         for (uint32_t k = 0; k < PT_STEPS; k++) {
@@ -221,67 +242,34 @@ __global__ void __launch_bounds__(PT_THREADS, 8) parse_tiles_kernel(ParseArgs a)
         __syncthreads();  // (c) list ready
 
         const uint32_t r_end = min(n_lines, r0 + PT_LIST);
-        if (warp == 0) {
-            if (!base_known) {
-                uint32_t nl_base = tile == 0 ? 0u : lb_sum_exclusive_wide(a.tile_status, tile, &a.stats->error);
-                if (lane == 0) {
-                    sm.nl_base = nl_base;
-                    if (tile != 0) st_relaxed_u64(a.tile_status + tile, (uint64_t)(nl_base + n_nl) | LB_PREFIX);
-                    if (tile == a.n_tiles - 1) {
-                        uint32_t total_nl = nl_base + n_nl;  // L = 1 + newlines before the last byte
-                        a.stats->line_count = 1u + total_nl - (a.text[N - 1] == '\n');
-                    }
-                }
-            }
-        } else {
-            for (uint32_t j = r0 + (tid - 32); j < r_end; j += PT_WORKERS) {
-                int32_t q = (int32_t)j - (int32_t)off;  // newline that precedes the line (-1: none)
-                uint32_t s = q < 0 ? 0u : sm.nl[q - w0] + 1u;  // tile-local
-                uint16_t pk = PK_NONE;
-                if (s < valid) {  // the final '\n' starts no line
-                    uint32_t e;
-                    bool known = true;
-                    if ((uint32_t)(q + 1) < n_nl) e = sm.nl[q + 1 - w0];
-                    else if (halo_first != NONE) e = halo_first;
-                    else if (valid < PT_TILE + PT_HALO) e = valid;  // the text ends in the staged bytes
-                    else known = false;                            // runs past the halo
-                    if (known) {
-                        uint32_t depth, cs, eff;
-                        uint32_t kind = classify_smem(sm.text, s, e, depth, cs, eff);
-                        pk = (uint16_t)(kind | (min(depth, 255u) << 8));
-                        if (kind != KIND_BLANK) my_max = max(my_max, depth);
-                    } else {
-                        pk = PK_FIXUP;
-                    }
-                }
-                sm.res_off[j - r0] = s;
-                sm.res_pk[j - r0] = pk;
-            }
-        }
-        __syncthreads();  // (d) base and results known
-        base_known = true;
-        const uint32_t nl_base = sm.nl_base;
-        // All threads write the round's lines in order: coalesced.
         for (uint32_t j = r0 + tid; j < r_end; j += PT_THREADS) {
-            uint16_t pk = sm.res_pk[j - r0];
-            if (pk == PK_NONE) continue;
+            int32_t q = (int32_t)j - (int32_t)off;  // newline that precedes the line (-1: none)
+            uint32_t s = q < 0 ? 0u : sm.nl[q - w0] + 1u;  // tile-local
+            if (s >= valid) continue;  // the final '\n' starts no line
             uint32_t idx = nl_base + j + 1 - off;
-            uint32_t start = (uint32_t)t0 + sm.res_off[j - r0];
             if (idx >= a.line_cap) {
                 atomicOr(&a.stats->error, OL_DEVERR_CAPACITY);
                 continue;
             }
-            a.offsets[idx] = start;
-            if (pk == PK_FIXUP) {
+            a.offsets[idx] = (uint32_t)t0 + s;
+            uint32_t e;
+            if ((uint32_t)(q + 1) < n_nl) e = sm.nl[q + 1 - w0];
+            else if (halo_first != NONE) e = halo_first;
+            else if (valid < PT_TILE + PT_HALO) e = valid;  // the text ends in the staged bytes
+            else {
+                // runs past the halo: classified by the fix-up kernel
                 uint32_t slot = atomicAdd(&a.stats->fixup_count, 1u);
-                if (slot < a.fixup_cap) a.fixup[slot] = make_uint2(idx, start);
+                if (slot < a.fixup_cap) a.fixup[slot] = make_uint2(idx, (uint32_t)t0 + s);
                 else atomicOr(&a.stats->error, OL_DEVERR_FIXUP);
                 continue;
             }
-            a.kinds[idx] = (uint8_t)(pk & 0xFF);
-            a.depth8[idx] = (uint8_t)(pk >> 8);
+            uint32_t depth;
+            uint32_t kind = classify_smem(sm.text, s, e, depth);
+            a.kinds[idx] = (uint8_t)kind;
+            a.depth8[idx] = (uint8_t)min(depth, 255u);
+            if (kind != KIND_BLANK) my_max = max(my_max, depth);
         }
-        __syncthreads();  // (e) the next round may overwrite the list and results
+        __syncthreads();  // (d) the next round may overwrite the list
     }
     for (int o = 16; o > 0; o >>= 1) my_max = max(my_max, __shfl_xor_sync(0xFFFFFFFFu, my_max, o));
     if (lane == 0 && my_max) atomicMax(&a.stats->max_content_depth, my_max);
@@ -331,8 +319,11 @@ __global__ void classify_lines_kernel(const uint8_t *__restrict__ text, uint64_t
 
 cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st) {
     if (a.n_tiles == 0) return cudaSuccess;
+    newline_count_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a.text, a.text_len, a.tile_count);
+    cudaError_t e = launch_scan_columns(a.tile_count, a.tile_base, nullptr, a.n_tiles, 1, 1, st);
+    if (e != cudaSuccess) return e;
     parse_tiles_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     uint32_t blocks = a.fixup_cap < 64 ? 8 : 64;
     parse_fixup_kernel<<<blocks, 256, 0, st>>>(a);

@@ -27,7 +27,7 @@ cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pa
     size_t total_bytes = 0;
     for (uint32_t i = 0; i < n; i++) total_bytes += (lens[i] + 15) & ~15u;
     cudaError_t e = ctx->pattern_dev.reserve(std::max<size_t>(total_bytes, 16), st);
-    if (e == cudaSuccess) e = ctx->scratch_a.reserve((size_t)n_tiles * kSearchMaxPatterns * 8, st);
+    if (e == cudaSuccess) e = ctx->scratch_a.reserve((size_t)n_tiles * kSearchMaxPatterns * 4 * 2, st);
     if (e != cudaSuccess) return e;
     // Patterns travel through pinned host staging so the copy is truly async
     // and the caller's buffers may be reused once this call returns.
@@ -61,8 +61,8 @@ cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pa
         a.text = d->text;
         a.text_len = d->text_len;
         a.n_tiles = n_tiles;
-        a.tile_status = (uint64_t *)ctx->scratch_a.ptr;
-        a.error = d_error;
+        a.counts = (uint32_t *)ctx->scratch_a.ptr;
+        a.bases = (uint32_t *)ctx->scratch_a.ptr + (size_t)n_tiles * kSearchMaxPatterns;
         uint32_t halo = 0;
         bool alone = halo_for(lens[i]) > kSearchMaxStagedPattern;
         uint32_t first = i;
@@ -80,8 +80,6 @@ cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pa
         }
         a.halo = halo;
         a.totals = d_totals + first;
-        if ((e = cudaMemsetAsync(a.tile_status, 0, (size_t)n_tiles * kSearchMaxPatterns * 8, st)) != cudaSuccess) return e;
-        if ((e = cudaMemsetAsync(a.totals, 0, (size_t)a.np * 4, st)) != cudaSuccess) return e;
         if ((e = launch_search(a, st)) != cudaSuccess) return e;
     }
     return cudaSuccess;

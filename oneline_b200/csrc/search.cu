@@ -1,20 +1,21 @@
 // Kernel (d): substring search, every overlapping occurrence, ascending.
 //
-// One launch searches up to eight patterns in one pass over the text. CTA b
-// owns the 16 KiB tile b and stages it, plus a halo of (longest pattern - 1)
-// bytes, in shared memory with 16-byte coalesced loads. For each pattern a
-// first-byte filter (byte SWAR over 16-byte pieces) queues candidate pieces per
-// warp; queued pieces are verified 32 at a time, one per lane: the last byte,
-// then every other byte, for all sixteen starts of the piece at once (byte
-// SWAR on shifted windows). An occurrence must end inside the text (the buffer
-// is zero padded: a pattern ending in NUL must not match the padding). The
-// match masks go to shared memory in position order; warp p then counts
-// pattern p's matches, runs the decoupled look-back over the tile match counts
-// of pattern p (the eight look-backs proceed in parallel) and writes the
-// pattern's first max_out offsets in ascending order through a staging buffer,
-// coalesced: no host sort, and a truncated result is the lowest max_out
-// offsets.
-//
+// Up to eight patterns are searched in one pass over the text; CTA b owns the
+// 16 KiB tile b and stages it, plus a halo of (longest pattern - 1) bytes, in
+// shared memory with 16-byte coalesced loads. For each pattern a first-byte
+// filter (byte SWAR over 16-byte pieces) queues candidate pieces per warp;
+// queued pieces are verified 32 at a time, one per lane: the last byte, then
+// every other byte, for all sixteen starts of the piece at once (byte SWAR on
+// shifted windows). An occurrence must end inside the text (the buffer is zero
+// padded: a pattern ending in NUL must not match the padding).
+// Three launches, no block waits on another:
+//   1. search_count_kernel: matches per (tile, pattern);
+//   2. scan_columns_kernel: per pattern, the first output slot of every tile
+//      and the total;
+//   3. search_write_kernel: tiles with matches recompute them for the patterns
+//      that have some and write every pattern's first max_out offsets in
+//      ascending order, coalesced through a staging buffer: no host sort, and
+//      a truncated result is the lowest max_out offsets.
 // Patterns longer than kSearchMaxStagedPattern run alone (np = 1) and read
 // their halo and verification bytes from global memory.
 //
@@ -30,14 +31,22 @@ namespace ol {
 
 constexpr uint32_t SR_THREADS = 256;
 constexpr uint32_t SR_STEPS = 4;
+constexpr uint32_t SR_PIECES = SR_THREADS * SR_STEPS;  // 16-byte pieces per tile
+constexpr uint32_t SR_QCAP = 160;                       // per-warp candidate queue (< 32 left + 128 per pattern)
 static_assert(SR_THREADS * 16 * SR_STEPS == kSearchTile, "search tile");
 
-constexpr uint32_t SR_QCAP = 160;  // per-warp candidate queue (< 32 left over + 128 per pattern)
+struct PatMeta {
+    const uint8_t *ptr;
+    uint32_t len;
+    uint32_t f4;  // first byte, replicated
+};
 
 struct SearchSmem {
-    alignas(16) uint8_t text[kSearchTile + kSearchMaxStagedPattern + 16];  // phase B: output staging
-    alignas(16) uint16_t match[kSearchMaxPatterns][SR_THREADS * SR_STEPS];  // per 16-byte piece, position order
+    alignas(16) uint8_t text[kSearchTile + kSearchMaxStagedPattern + 16];  // write pass: output staging after use
     uint16_t queue[SR_THREADS / 32][SR_QCAP];  // (pattern << 10) | piece, per warp
+    PatMeta pat[kSearchMaxPatterns];
+    uint32_t count[kSearchMaxPatterns];
+    uint32_t active;  // write pass: patterns with matches in this tile (bit mask)
 };
 
 // 16 bytes of shared memory starting at any byte offset.
@@ -73,16 +82,16 @@ __device__ __forceinline__ uint32_t gather16(uint32_t c0, uint32_t c1, uint32_t 
     return g(c0) | (g(c1) << 4) | (g(c2) << 8) | (g(c3) << 12);
 }
 
-// Exact matches of pattern p at the sixteen starts of one piece: first byte,
-// then the last byte, then every other byte, all sixteen starts at once.
-__device__ __forceinline__ uint32_t verify_piece(const SearchArgs &a, const SearchSmem &sm, uint32_t p, uint32_t piece,
-                                                 bool staged, bool tail_tile, uint64_t t0) {
-    const uint32_t m = a.pat_len[p];
-    const uint8_t *pat = a.pat[p];
-    const uint32_t F4 = __ldg(pat) * 0x01010101u;
-    const uint32_t lo = piece * 16;  // position order: piece x covers tile bytes [16x, 16x+16)
+// Exact matches of a pattern at the sixteen starts of one piece (piece x
+// covers tile bytes [16x, 16x+16)): first byte, then the last byte, then every
+// other byte, all sixteen starts at once.
+__device__ __forceinline__ uint32_t verify_piece(const SearchArgs &a, const SearchSmem &sm, const PatMeta &pm,
+                                                 uint32_t piece, bool staged, bool tail_tile, uint64_t t0) {
+    const uint32_t m = pm.len;
+    const uint32_t lo = piece * 16;
     const uint4 v = *reinterpret_cast<const uint4 *>(&sm.text[lo]);
-    uint32_t c0 = zero_bytes(v.x ^ F4), c1 = zero_bytes(v.y ^ F4), c2 = zero_bytes(v.z ^ F4), c3 = zero_bytes(v.w ^ F4);
+    uint32_t c0 = zero_bytes(v.x ^ pm.f4), c1 = zero_bytes(v.y ^ pm.f4);
+    uint32_t c2 = zero_bytes(v.z ^ pm.f4), c3 = zero_bytes(v.w ^ pm.f4);
     if (tail_tile) {  // starts past N - m cannot match
         const int64_t last_ok = (int64_t)a.text_len - (int64_t)m - (int64_t)t0;
         uint32_t keep[4];
@@ -98,7 +107,7 @@ __device__ __forceinline__ uint32_t verify_piece(const SearchArgs &a, const Sear
     }
     for (uint32_t jj = 1; jj < m && (c0 | c1 | c2 | c3); jj++) {
         const uint32_t j = jj == 1 ? m - 1 : jj - 1;  // last byte first, then 1, 2, ...
-        const uint32_t P4 = __ldg(pat + j) * 0x01010101u;
+        const uint32_t P4 = __ldg(pm.ptr + j) * 0x01010101u;
         uint4 w = window16(sm.text, lo + j, staged, a.text, t0, a.text_len);
         c0 &= zero_bytes(w.x ^ P4);
         c1 &= zero_bytes(w.y ^ P4);
@@ -108,15 +117,10 @@ __device__ __forceinline__ uint32_t verify_piece(const SearchArgs &a, const Sear
     return gather16(c0, c1, c2, c3);
 }
 
-__global__ void __launch_bounds__(SR_THREADS) search_kernel(SearchArgs a) {
-    __shared__ SearchSmem sm;
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t tile = blockIdx.x;
-    const uint64_t t0 = (uint64_t)tile * kSearchTile;
-    const uint64_t N = a.text_len;
+// Loads tile b (plus the halo) into shared memory and the pattern table.
+__device__ __forceinline__ void load_tile(const SearchArgs &a, SearchSmem &sm, uint64_t t0, uint4 v[SR_STEPS]) {
+    const uint32_t tid = threadIdx.x;
     const bool staged = a.halo <= kSearchMaxStagedPattern;
-
-    uint4 v[SR_STEPS];
 #pragma unroll
     for (uint32_t k = 0; k < SR_STEPS; k++) v[k] = ld_stream16(a.text + t0 + k * 4096 + tid * 16);
 #pragma unroll
@@ -125,28 +129,48 @@ __global__ void __launch_bounds__(SR_THREADS) search_kernel(SearchArgs a) {
     for (uint32_t o = tid * 16; o < halo; o += SR_THREADS * 16)
         *reinterpret_cast<uint4 *>(&sm.text[kSearchTile + o]) = ld_stream16(a.text + t0 + kSearchTile + o);
     if (tid == 0) *reinterpret_cast<uint4 *>(&sm.text[kSearchTile + halo]) = make_uint4(0, 0, 0, 0);
-    // clear the match masks of every pattern (64 bytes per thread)
-    for (uint32_t o = tid; o < kSearchMaxPatterns * SR_THREADS * SR_STEPS / 8; o += SR_THREADS)
-        reinterpret_cast<uint4 *>(&sm.match[0][0])[o] = make_uint4(0, 0, 0, 0);
-    __syncthreads();
+    if (tid < a.np) {
+        PatMeta pm;
+        pm.ptr = a.pat[tid];
+        pm.len = a.pat_len[tid];
+        pm.f4 = __ldg(pm.ptr) * 0x01010101u;
+        sm.pat[tid] = pm;
+        sm.count[tid] = 0;
+    }
+}
 
-    // Phase A. Every lane runs the first-byte filter (loose byte SWAR, three
-    // operations per word) on its four pieces for each pattern; pieces with a
-    // candidate go to the warp's queue, and every 32 queued pieces are verified
-    // together, one per lane, so that verification work follows the number of
-    // candidates rather than the number of pieces.
-    const bool tail_tile = t0 + kSearchTile + a.halo + 16 > N;
+// Runs the filter of every pattern in `mask` over the tile: every lane tests
+// its four pieces with the loose first-byte SWAR (three operations per word);
+// pieces with a candidate are queued per warp and verified 32 at a time, one
+// per lane, so verification work follows the number of candidates. `sink(p,
+// piece, matches)` receives every verified piece (matches may be 0).
+template <class Sink>
+__device__ __forceinline__ void filter_tile(const SearchArgs &a, SearchSmem &sm, const uint4 v[SR_STEPS], uint32_t mask,
+                                            uint64_t t0, Sink sink) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool staged = a.halo <= kSearchMaxStagedPattern;
+    const bool tail_tile = t0 + kSearchTile + a.halo + 16 > a.text_len;
     uint16_t *queue = sm.queue[warp];
     uint32_t qn = 0;  // queued entries (the same in every lane)
+    auto drain = [&](uint32_t n) {
+        for (uint32_t done = 0; done < n; done += 32) {
+            if (done + lane < n) {
+                uint32_t e = queue[done + lane];
+                uint32_t p = e >> 10, piece = e & 1023u;
+                sink(p, piece, verify_piece(a, sm, sm.pat[p], piece, staged, tail_tile, t0));
+            }
+        }
+    };
 #pragma unroll 1
     for (uint32_t p = 0; p < a.np; p++) {
-        const uint32_t F4 = __ldg(a.pat[p]) * 0x01010101u;
+        if (!((mask >> p) & 1u)) continue;
+        const uint32_t F4 = sm.pat[p].f4;
         uint32_t cm = 0;
 #pragma unroll
         for (uint32_t k = 0; k < SR_STEPS; k++) {
             uint32_t c = zero_bytes_loose(v[k].x ^ F4) | zero_bytes_loose(v[k].y ^ F4) | zero_bytes_loose(v[k].z ^ F4) |
                          zero_bytes_loose(v[k].w ^ F4);
-            cm |= (c != 0) << k;
+            cm |= (uint32_t)(c != 0) << k;
         }
         uint32_t n = __popc(cm), inc = n;
 #pragma unroll
@@ -163,74 +187,75 @@ __global__ void __launch_bounds__(SR_THREADS) search_kernel(SearchArgs a) {
         qn += __shfl_sync(0xFFFFFFFFu, inc, 31);
         __syncwarp();
         if (qn >= 32) {
-            uint32_t done = 0;
-            for (; done + 32 <= qn; done += 32) {
-                uint32_t e = queue[done + lane];
-                uint32_t piece = e & 1023u;
-                sm.match[e >> 10][piece] = (uint16_t)verify_piece(a, sm, e >> 10, piece, staged, tail_tile, t0);
-            }
-            uint32_t rem = qn - done;
-            uint16_t keep = lane < rem ? queue[done + lane] : (uint16_t)0;
+            uint32_t full = qn & ~31u;
+            drain(full);
+            uint32_t rem = qn - full;
+            uint16_t keep = lane < rem ? queue[full + lane] : (uint16_t)0;
             __syncwarp();
             if (lane < rem) queue[lane] = keep;
             qn = rem;
             __syncwarp();
         }
     }
-    if (lane < qn) {
-        uint32_t e = queue[lane];
-        uint32_t piece = e & 1023u;
-        sm.match[e >> 10][piece] = (uint16_t)verify_piece(a, sm, e >> 10, piece, staged, tail_tile, t0);
-    }
-    __syncthreads();
+    drain(qn);
+}
 
-    // Phase B: warp p counts, looks back and writes pattern p on its own.
-    // Lane l owns pieces [32 l, 32 l + 32) of the tile, in position order.
-    if (warp >= a.np) return;
+// Pass 1: matches of every pattern in every tile (counts only).
+__global__ void __launch_bounds__(SR_THREADS) search_count_kernel(SearchArgs a) {
+    __shared__ SearchSmem sm;
+    const uint32_t tid = threadIdx.x;
+    const uint64_t t0 = (uint64_t)blockIdx.x * kSearchTile;
+    uint4 v[SR_STEPS];
+    load_tile(a, sm, t0, v);
+    __syncthreads();
+    filter_tile(a, sm, v, 0xFFu, t0, [&](uint32_t p, uint32_t piece, uint32_t mk) {
+        if (mk) atomicAdd(&sm.count[p], __popc(mk));
+    });
+    __syncthreads();
+    if (tid < a.np) a.counts[(size_t)blockIdx.x * kSearchMaxPatterns + tid] = sm.count[tid];
+}
+
+// Pass 3: tiles with matches recompute the match masks of the patterns that
+// have some, then warp p writes pattern p's matches at the offsets from the
+// scan of pass 2, in position order, through a 2 KiB staging buffer so that
+// the stores are coalesced. Tiles without matches exit before loading text.
+__global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) {
+    __shared__ SearchSmem sm;
+    __shared__ uint16_t match[kSearchMaxPatterns][SR_PIECES];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t tile = blockIdx.x;
+    const uint64_t t0 = (uint64_t)tile * kSearchTile;
+    // patterns with matches here whose output window is not yet full
+    uint32_t want = 0;
+    for (uint32_t p = 0; p < a.np; p++) {
+        size_t at = (size_t)tile * kSearchMaxPatterns + p;
+        if (a.counts[at] && a.bases[at] < a.max_out[p]) want |= 1u << p;
+    }
+    if (!want) return;
+    uint4 v[SR_STEPS];
+    load_tile(a, sm, t0, v);
+    for (uint32_t o = tid; o < kSearchMaxPatterns * SR_PIECES / 8; o += SR_THREADS)
+        reinterpret_cast<uint4 *>(&match[0][0])[o] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    filter_tile(a, sm, v, want, t0, [&](uint32_t p, uint32_t piece, uint32_t mk) { match[p][piece] = (uint16_t)mk; });
+    __syncthreads();
+    if (warp >= a.np || !((want >> warp) & 1u)) return;
     const uint32_t p = warp;
-    const uint4 *row = reinterpret_cast<const uint4 *>(&sm.match[p][lane * 32]);
-    uint32_t cnt = 0;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        uint4 r = row[q];  // 8 pieces
-        cnt += __popc(r.x) + __popc(r.y) + __popc(r.z) + __popc(r.w);
-    }
-    uint32_t inc = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
-        if ((int)lane >= o) inc += t;
-    }
-    const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
-    uint64_t *st = a.tile_status + (uint64_t)tile * kSearchMaxPatterns + p;
-    if (lane == 0) st_relaxed_u64(st, (uint64_t)total | (tile == 0 ? LB_PREFIX : LB_AGGREGATE));
-    const uint32_t base =
-        tile == 0 ? 0u : lb_sum_exclusive_wide(a.tile_status + p, tile, a.error, kSearchMaxPatterns);
-    if (lane == 0) {
-        if (tile != 0) st_relaxed_u64(st, (uint64_t)(base + total) | LB_PREFIX);
-        if (tile == a.n_tiles - 1) a.totals[p] = base + total;
-    }
     const uint32_t max_out = a.max_out[p];
-    if (total == 0 || base >= max_out) return;
-    // Ordered, coalesced output: chunk c is lane c's 32 pieces; its matches are
-    // expanded into this warp's 2 KiB of staging, then copied out by all lanes.
+    uint32_t run = a.bases[(size_t)tile * kSearchMaxPatterns + p];  // first output slot of this tile
     uint32_t *out = a.out[p];
     uint32_t *stg = reinterpret_cast<uint32_t *>(sm.text) + warp * 512;
-    const uint32_t excl = inc - cnt;
-    uint32_t nz = __ballot_sync(0xFFFFFFFFu, cnt != 0);
-    while (nz) {
-        const uint32_t c = __ffs(nz) - 1;
-        nz &= nz - 1;
-        const uint32_t c_base = base + __shfl_sync(0xFFFFFFFFu, excl, c);  // first output slot of the chunk
-        const uint32_t c_total = __shfl_sync(0xFFFFFFFFu, cnt, c);
-        if (c_base >= max_out) break;
+    // chunk c = pieces [32c, 32c+32), one per lane
+    for (uint32_t c = 0; c < SR_PIECES / 32 && run < max_out; c++) {
         const uint32_t piece = c * 32 + lane;
-        uint32_t mk = sm.match[p][piece], n = __popc(mk), pi = n;
+        uint32_t mk = match[p][piece], n = __popc(mk), pi = n;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             uint32_t t = __shfl_up_sync(0xFFFFFFFFu, pi, o);
             if ((int)lane >= o) pi += t;
         }
+        const uint32_t c_total = __shfl_sync(0xFFFFFFFFu, pi, 31);
+        if (c_total == 0) continue;
         uint32_t w = pi - n;
         while (mk) {
             uint32_t b = __ffs(mk) - 1;
@@ -238,14 +263,18 @@ __global__ void __launch_bounds__(SR_THREADS) search_kernel(SearchArgs a) {
             stg[w++] = (uint32_t)(t0 + piece * 16 + b);
         }
         __syncwarp();
-        for (uint32_t i = lane; i < c_total && c_base + i < max_out; i += 32) out[c_base + i] = stg[i];
+        for (uint32_t i = lane; i < c_total && run + i < max_out; i += 32) out[run + i] = stg[i];
+        run += c_total;
         __syncwarp();
     }
 }
 
 cudaError_t launch_search(const SearchArgs &a, cudaStream_t st) {
     if (a.n_tiles == 0 || a.np == 0) return cudaSuccess;
-    search_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a);
+    search_count_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a);
+    cudaError_t e = launch_scan_columns(a.counts, a.bases, a.totals, a.n_tiles, a.np, kSearchMaxPatterns, st);
+    if (e != cudaSuccess) return e;
+    search_write_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }
 
