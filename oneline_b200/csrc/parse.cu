@@ -47,36 +47,45 @@ __device__ __forceinline__ uint32_t lds4(const uint8_t *base, uint32_t off) {
     return __funnelshift_r(w[0], w[1], (off & 3) * 8);
 }
 
-// High bits of the bytes of w equal to '|' and to a blank (' ' or '\t').
+// High bit of every byte of w equal to '|'.
 __device__ __forceinline__ uint32_t pipe_bits(uint32_t w) { return zero_bytes(w ^ 0x7C7C7C7Cu); }
-__device__ __forceinline__ uint32_t blank_bits(uint32_t w) {
-    return zero_bytes(w ^ 0x20202020u) | zero_bytes(w ^ 0x09090909u);
-}
 
 // parse_line (crates/oneline-simd/src/line.rs:8-44) for a line held in shared
 // memory at tile-local [s, e), e = its '\n' or the text end; the bytes from e
-// to e+3 are readable. Same rules as classify_line, four bytes per step.
+// to e+3 are readable. The prefix is read as alternating runs: a run of '|'
+// four bytes per step (byte SWAR), then a run of blanks; it continues only
+// while another '|' follows the blanks.
 __device__ __forceinline__ uint32_t classify_smem(const uint8_t *t, uint32_t s, uint32_t e, uint32_t &depth_out) {
     uint32_t eff = e;
     while (eff > s && t[eff - 1] == '\r') eff--;
     uint32_t c = s, depth = 0;
-    const bool piped = t[s] == '|' && s < eff;
-    for (;;) {
-        uint32_t w = lds4(t, c);
-        uint32_t hp = piped ? pipe_bits(w) : 0u;
-        uint32_t other = ~(hp | blank_bits(w)) & 0x80808080u;
-        if (other) {
-            uint32_t nb = (__ffs(other) - 8) >> 3;  // first byte that ends the prefix
-            depth += __popc(hp & ((1u << (8 * nb)) - 1u));
-            c += nb;
+    if (s < eff && t[s] == '|') {
+        for (;;) {
+            // run of '|' (stops at a non-'|' byte, at the latest at eff)
+            for (;;) {
+                uint32_t other = ~pipe_bits(lds4(t, c)) & 0x80808080u;
+                if (other) {
+                    uint32_t nb = (__ffs(other) - 8) >> 3;
+                    depth += nb;
+                    c += nb;
+                    break;
+                }
+                depth += 4;
+                c += 4;
+            }
+            // run of blanks; the prefix goes on only if a '|' follows it
+            uint32_t b = c;
+            while (b < eff && is_blank(t[b])) b++;
+            if (b < eff && t[b] == '|') {
+                c = b;
+                continue;
+            }
+            c = b;
             break;
         }
-        depth += __popc(hp);
-        c += 4;
+    } else {
+        while (c < eff && is_blank(t[c])) c++;
     }
-    // a prefix never runs into the '\r' / '\n' run, but a blank-only run may
-    // be followed by nothing: clamp to eff
-    if (c > eff) c = eff;
     depth_out = depth;
     if (c >= eff) return KIND_BLANK;
     uint32_t w = lds4(t, c);
@@ -135,7 +144,7 @@ __global__ void __launch_bounds__(PT_THREADS) newline_count_kernel(const uint8_t
 // from the scan of pass 2. Consecutive threads take consecutive lines, so the
 // outputs are written coalesced. A line that runs past the tile plus a
 // 256-byte halo is queued for the fix-up kernel.
-__global__ void __launch_bounds__(PT_THREADS, 8) parse_tiles_kernel(ParseArgs a) {
+__global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a) {
     __shared__ ParseSmem sm;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;

@@ -208,8 +208,12 @@ __global__ void __launch_bounds__(SR_THREADS) search_count_kernel(SearchArgs a) 
     uint4 v[SR_STEPS];
     load_tile(a, sm, t0, v);
     __syncthreads();
+    // Lanes verifying pieces of the same pattern add up their matches first:
+    // one shared-memory atomic per (round, pattern) instead of one per piece.
     filter_tile(a, sm, v, 0xFFu, t0, [&](uint32_t p, uint32_t piece, uint32_t mk) {
-        if (mk) atomicAdd(&sm.count[p], __popc(mk));
+        const uint32_t group = __match_any_sync(__activemask(), p);
+        const uint32_t sum = __reduce_add_sync(group, __popc(mk));
+        if ((threadIdx.x & 31) == __ffs(group) - 1 && sum) atomicAdd(&sm.count[p], sum);
     });
     __syncthreads();
     if (tid < a.np) a.counts[(size_t)blockIdx.x * kSearchMaxPatterns + tid] = sm.count[tid];
