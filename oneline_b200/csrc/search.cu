@@ -14,8 +14,9 @@
 //      and the total;
 //   3. search_write_kernel: tiles with matches recompute them for the patterns
 //      that have some and write every pattern's first max_out offsets in
-//      ascending order, coalesced through a staging buffer: no host sort, and
-//      a truncated result is the lowest max_out offsets.
+//      ascending order, the whole block writing one contiguous range per
+//      pattern: no host sort, and a truncated result is the lowest max_out
+//      offsets.
 // Patterns longer than kSearchMaxStagedPattern run alone (np = 1) and read
 // their halo and verification bytes from global memory.
 //
@@ -220,12 +221,15 @@ __global__ void __launch_bounds__(SR_THREADS) search_count_kernel(SearchArgs a) 
 }
 
 // Pass 3: tiles with matches recompute the match masks of the patterns that
-// have some, then warp p writes pattern p's matches at the offsets from the
-// scan of pass 2, in position order, through a 2 KiB staging buffer so that
-// the stores are coalesced. Tiles without matches exit before loading text.
+// have some; then, pattern by pattern, thread t takes pieces [4t, 4t+4) (in
+// position order), a block scan of the per-thread match counts gives every
+// thread its first output slot after the tile's base from pass 2, and each
+// thread writes its matches there: the block's stores cover one contiguous
+// range. Tiles without matches exit before loading text.
 __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) {
     __shared__ SearchSmem sm;
     __shared__ uint16_t match[kSearchMaxPatterns][SR_PIECES];
+    __shared__ uint32_t warp_sum[SR_THREADS / 32];
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;
     const uint64_t t0 = (uint64_t)tile * kSearchTile;
@@ -243,33 +247,35 @@ __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) 
     __syncthreads();
     filter_tile(a, sm, v, want, t0, [&](uint32_t p, uint32_t piece, uint32_t mk) { match[p][piece] = (uint16_t)mk; });
     __syncthreads();
-    if (warp >= a.np || !((want >> warp) & 1u)) return;
-    const uint32_t p = warp;
-    const uint32_t max_out = a.max_out[p];
-    uint32_t run = a.bases[(size_t)tile * kSearchMaxPatterns + p];  // first output slot of this tile
-    uint32_t *out = a.out[p];
-    uint32_t *stg = reinterpret_cast<uint32_t *>(sm.text) + warp * 512;
-    // chunk c = pieces [32c, 32c+32), one per lane
-    for (uint32_t c = 0; c < SR_PIECES / 32 && run < max_out; c++) {
-        const uint32_t piece = c * 32 + lane;
-        uint32_t mk = match[p][piece], n = __popc(mk), pi = n;
+    for (uint32_t w = want; w; w &= w - 1) {
+        const uint32_t p = __ffs(w) - 1;
+        const uint2 m4 = *reinterpret_cast<const uint2 *>(&match[p][4 * tid]);  // my 4 pieces
+        const uint32_t n = __popc(m4.x) + __popc(m4.y), inc0 = n;
+        uint32_t inc = inc0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xFFFFFFFFu, pi, o);
-            if ((int)lane >= o) pi += t;
+            uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if ((int)lane >= o) inc += t;
         }
-        const uint32_t c_total = __shfl_sync(0xFFFFFFFFu, pi, 31);
-        if (c_total == 0) continue;
-        uint32_t w = pi - n;
-        while (mk) {
-            uint32_t b = __ffs(mk) - 1;
-            mk &= mk - 1;
-            stg[w++] = (uint32_t)(t0 + piece * 16 + b);
+        if (lane == 31) warp_sum[warp] = inc;
+        __syncthreads();
+        uint32_t before = 0;
+        for (uint32_t x = 0; x < warp; x++) before += warp_sum[x];
+        uint32_t r = a.bases[(size_t)tile * kSearchMaxPatterns + p] + before + inc - n;
+        const uint32_t max_out = a.max_out[p];
+        uint32_t *out = a.out[p];
+        const uint32_t mm[2] = {m4.x, m4.y};
+#pragma unroll
+        for (uint32_t h = 0; h < 2; h++) {
+            uint32_t bits = mm[h];  // pieces 4t+2h (low 16 bits) and 4t+2h+1 (high 16 bits)
+            while (bits && r < max_out) {
+                uint32_t b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                uint32_t piece = 4 * tid + 2 * h + (b >> 4);
+                out[r++] = (uint32_t)(t0 + piece * 16 + (b & 15));
+            }
         }
-        __syncwarp();
-        for (uint32_t i = lane; i < c_total && run + i < max_out; i += 32) out[run + i] = stg[i];
-        run += c_total;
-        __syncwarp();
+        __syncthreads();  // warp_sum is reused by the next pattern
     }
 }
 
