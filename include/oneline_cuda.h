@@ -153,6 +153,38 @@ ol_status ol_search_multi(ol_ctx *ctx, const ol_doc *doc, const uint8_t *const *
 ol_status ol_search_multi_async(ol_ctx *ctx, const ol_doc *doc, const uint8_t *const *patterns, const uint32_t *lens,
                                 uint32_t n, const uint32_t *max_matches, uint32_t *d_totals, uint32_t *const *d_outs);
 
+/* ---- substring search that allocates nothing. No counterpart in the
+ *      reference: an addition for callers that cannot call cudaMalloc, such as a
+ *      serving process whose own allocator reserved the GPU's memory up front, or
+ *      a latency-critical loop that must not stall the device on cudaMalloc /
+ *      cudaFree. It takes no context: everything is the caller's except one fixed
+ *      scratch array of 1 MiB + 256 B inside this library, which every GPU that
+ *      loads the library holds until the process exits.
+ *
+ *   d_text      device text, 16-byte aligned, at most OL_NOALLOC_MAX_TEXT_LEN
+ *               bytes; longer texts are refused with OL_ERR_INPUT_TOO_LARGE.
+ *   text_cap    bytes readable at d_text, at least OL_NOALLOC_TEXT_CAP(text_len)
+ *               (whole 16 KiB tiles plus 64 bytes; what lies past text_len is
+ *               read but never matched, so it may hold anything).
+ *   pattern     host memory, 1..OL_MAX_PATTERN_LEN bytes, copied before return.
+ *   d_total     device u32: the number of occurrences.
+ *   d_out       device u32[max_matches]: the first min(total, max_matches)
+ *               offsets, ascending (may be NULL when max_matches is 0).
+ *   stream      a cudaStream_t (NULL: the legacy default stream); the call only
+ *               enqueues, results are ready when the stream reaches them.
+ *   err/err_cap optional buffer for a message when the status is not OL_OK.
+ *
+ * Call it with the device that owns the buffers current. The first call on a
+ * device looks up the scratch array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture. Every call on a device uses
+ * the same scratch array: calls that overlap on the GPU (on streams with no
+ * ordering between them) race and may return wrong results. */
+#define OL_NOALLOC_MAX_TEXT_LEN (256ull << 20)
+#define OL_NOALLOC_TEXT_CAP(len) ((((uint64_t)(len) + 16383ull) / 16384ull) * 16384ull + 64ull)
+ol_status ol_search_noalloc(const uint8_t *d_text, uint64_t text_len, uint64_t text_cap, const uint8_t *pattern,
+                            uint32_t pat_len, uint32_t max_matches, uint32_t *d_total, uint32_t *d_out, void *stream,
+                            char *err, uint32_t err_cap);
+
 #ifdef __cplusplus
 }
 #endif
