@@ -126,6 +126,7 @@ extern "C" ol_status ol_search_noalloc(const uint8_t *d_text, uint64_t text_len,
     a.pat_len[0] = pat_len;
     a.out[0] = d_out;
     a.max_out[0] = max_matches;
+    a.ld = ol::scan_ld(a.n_tiles);
     a.counts = reinterpret_cast<uint32_t *>(scratch + kPatternBytes);
     a.bases = a.counts + kColumnWords;
     a.totals = d_total;

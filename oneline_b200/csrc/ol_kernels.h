@@ -32,10 +32,14 @@ struct ParseArgs {
 
 cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st);
 
-// Exclusive scan of the first `cols` columns of a row-major [rows][stride] u32
-// matrix (one block per column); totals[c] (optional) receives column c's sum.
+// Exclusive scan of each of `cols` columns of a column-major u32 matrix:
+// column c is `rows` entries at in + c * ld (in, out 16-byte aligned, ld a
+// multiple of 4); out has the same layout; totals[c] (optional) receives
+// column c's sum.
 cudaError_t launch_scan_columns(const uint32_t *in, uint32_t *out, uint32_t *totals, uint32_t rows, uint32_t cols,
-                                uint32_t stride, cudaStream_t st);
+                                uint32_t ld, cudaStream_t st);
+// Column stride for per-tile count columns: rows rounded up to a multiple of 4.
+inline uint32_t scan_ld(uint32_t rows) { return (rows + 3u) & ~3u; }
 cudaError_t launch_classify_lines(const uint8_t *text, uint64_t N, const uint32_t *offsets, uint32_t L, FlatNode *nodes,
                                   uint32_t *depth32, cudaStream_t st);
 
@@ -87,8 +91,9 @@ struct SearchArgs {
     uint32_t pat_len[kSearchMaxPatterns];
     uint32_t *out[kSearchMaxPatterns];          // ascending offsets, first max_out[p] of them
     uint32_t max_out[kSearchMaxPatterns];
-    uint32_t *counts;        // [n_tiles][kSearchMaxPatterns] matches per tile (pass 1)
-    uint32_t *bases;         // [n_tiles][kSearchMaxPatterns] exclusive scans (pass 2)
+    uint32_t ld;             // column stride of counts and bases: scan_ld(n_tiles)
+    uint32_t *counts;        // [np][ld] matches per tile (pass 1), 16-byte aligned
+    uint32_t *bases;         // [np][ld] exclusive scans (pass 2), 16-byte aligned
     uint32_t *totals;        // kSearchMaxPatterns totals (pass 2)
 };
 

@@ -329,7 +329,7 @@ __global__ void classify_lines_kernel(const uint8_t *__restrict__ text, uint64_t
 cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st) {
     if (a.n_tiles == 0) return cudaSuccess;
     newline_count_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a.text, a.text_len, a.tile_count);
-    cudaError_t e = launch_scan_columns(a.tile_count, a.tile_base, nullptr, a.n_tiles, 1, 1, st);
+    cudaError_t e = launch_scan_columns(a.tile_count, a.tile_base, nullptr, a.n_tiles, 1, scan_ld(a.n_tiles), st);
     if (e != cudaSuccess) return e;
     parse_tiles_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a);
     e = cudaGetLastError();

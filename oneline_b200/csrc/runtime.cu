@@ -191,14 +191,14 @@ cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d) {
     cudaStream_t st = ctx->stream;
     cudaError_t e;
     uint32_t n_tiles = parse_tiles(d->text_len);
-    if ((e = ctx->scratch_a.reserve((size_t)n_tiles * 8, st)) != cudaSuccess) return e;
+    if ((e = ctx->scratch_a.reserve((size_t)scan_ld(n_tiles) * 8, st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(d->stats, 0, sizeof(DocStats), st)) != cudaSuccess) return e;
     ParseArgs a{};
     a.text = d->text;
     a.text_len = d->text_len;
     a.n_tiles = n_tiles;
     a.tile_count = (uint32_t *)ctx->scratch_a.ptr;
-    a.tile_base = (uint32_t *)ctx->scratch_a.ptr + n_tiles;
+    a.tile_base = (uint32_t *)ctx->scratch_a.ptr + scan_ld(n_tiles);  // 16-byte aligned
     a.stats = d->stats;
     a.offsets = d->offsets;
     a.kinds = d->kinds;

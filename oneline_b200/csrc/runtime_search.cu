@@ -27,7 +27,7 @@ cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pa
     size_t total_bytes = 0;
     for (uint32_t i = 0; i < n; i++) total_bytes += (lens[i] + 15) & ~15u;
     cudaError_t e = ctx->pattern_dev.reserve(std::max<size_t>(total_bytes, 16), st);
-    if (e == cudaSuccess) e = ctx->scratch_a.reserve((size_t)n_tiles * kSearchMaxPatterns * 4 * 2, st);
+    if (e == cudaSuccess) e = ctx->scratch_a.reserve((size_t)scan_ld(n_tiles) * kSearchMaxPatterns * 4 * 2, st);
     if (e != cudaSuccess) return e;
     // Patterns travel through pinned host staging so the copy is truly async
     // and the caller's buffers may be reused once this call returns.
@@ -61,8 +61,9 @@ cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pa
         a.text = d->text;
         a.text_len = d->text_len;
         a.n_tiles = n_tiles;
+        a.ld = scan_ld(n_tiles);
         a.counts = (uint32_t *)ctx->scratch_a.ptr;
-        a.bases = (uint32_t *)ctx->scratch_a.ptr + (size_t)n_tiles * kSearchMaxPatterns;
+        a.bases = (uint32_t *)ctx->scratch_a.ptr + (size_t)a.ld * kSearchMaxPatterns;
         uint32_t halo = 0;
         bool alone = halo_for(lens[i]) > kSearchMaxStagedPattern;
         uint32_t first = i;

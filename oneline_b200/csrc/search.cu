@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(SR_THREADS) search_count_kernel(SearchArgs a) 
         if ((threadIdx.x & 31) == __ffs(group) - 1 && sum) atomicAdd(&sm.count[p], sum);
     });
     __syncthreads();
-    if (tid < a.np) a.counts[(size_t)blockIdx.x * kSearchMaxPatterns + tid] = sm.count[tid];
+    if (tid < a.np) a.counts[(size_t)tid * a.ld + blockIdx.x] = sm.count[tid];
 }
 
 // Pass 3: tiles with matches recompute the match masks of the patterns that
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) 
     // patterns with matches here whose output window is not yet full
     uint32_t want = 0;
     for (uint32_t p = 0; p < a.np; p++) {
-        size_t at = (size_t)tile * kSearchMaxPatterns + p;
+        size_t at = (size_t)p * a.ld + tile;
         if (a.counts[at] && a.bases[at] < a.max_out[p]) want |= 1u << p;
     }
     if (!want) return;
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) 
         __syncthreads();
         uint32_t before = 0;
         for (uint32_t x = 0; x < warp; x++) before += warp_sum[x];
-        uint32_t r = a.bases[(size_t)tile * kSearchMaxPatterns + p] + before + inc - n;
+        uint32_t r = a.bases[(size_t)p * a.ld + tile] + before + inc - n;
         const uint32_t max_out = a.max_out[p];
         uint32_t *out = a.out[p];
         const uint32_t mm[2] = {m4.x, m4.y};
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) 
 cudaError_t launch_search(const SearchArgs &a, cudaStream_t st) {
     if (a.n_tiles == 0 || a.np == 0) return cudaSuccess;
     search_count_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a);
-    cudaError_t e = launch_scan_columns(a.counts, a.bases, a.totals, a.n_tiles, a.np, kSearchMaxPatterns, st);
+    cudaError_t e = launch_scan_columns(a.counts, a.bases, a.totals, a.n_tiles, a.np, a.ld, st);
     if (e != cudaSuccess) return e;
     search_write_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a);
     return cudaGetLastError();
