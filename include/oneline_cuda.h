@@ -153,6 +153,32 @@ ol_status ol_search_multi(ol_ctx *ctx, const ol_doc *doc, const uint8_t *const *
 ol_status ol_search_multi_async(ol_ctx *ctx, const ol_doc *doc, const uint8_t *const *patterns, const uint32_t *lens,
                                 uint32_t n, const uint32_t *max_matches, uint32_t *d_totals, uint32_t *const *d_outs);
 
+/* ---- dictionary search: GpuParser::compile_patterns / search_many,
+ *      GpuPatternSet::{len, is_empty} (crates/oneline-gpu/src/many.rs:139-176,
+ *      391-399). A set holds 1..OL_MAX_DICT_PATTERNS patterns of
+ *      OL_MIN_SET_PATTERN_LEN..OL_MAX_SET_PATTERN_LEN bytes (the reference caps
+ *      the count at OL_MAX_PATTERNS; the drop-in wrappers apply that cap).
+ *      Results follow ManyResult (many.rs:84-94): counts[i] per pattern, the
+ *      total, and the first min(total, max_hits) hits in (pattern, offset)
+ *      order, the order of ManyPatterns::find_all (oneline-simd
+ *      search.rs:259-282). Identical patterns are reported once per id. `doc`
+ *      may be NULL: the compiled set does not depend on the document. */
+#define OL_MAX_DICT_PATTERNS 65536u
+ol_status ol_patset_compile(ol_ctx *ctx, const ol_doc *doc, const uint8_t *const *patterns, const uint32_t *lens,
+                            uint32_t n, ol_patset **out);
+void ol_patset_free(ol_patset *set);
+uint32_t ol_patset_len(const ol_patset *set);
+/* Distinct patterns in the set. */
+uint32_t ol_patset_unique(const ol_patset *set);
+ol_status ol_search_many(ol_ctx *ctx, const ol_doc *doc, const ol_patset *set, uint64_t max_hits, uint32_t *counts,
+                         uint64_t *total_hits, ol_hit *hits);
+/* Same, with the hits left in device memory (d_hits holds max_hits entries);
+ * counts and *total_hits are host outputs. heavy_min_hits: patterns expected
+ * to occur at least this often are collected as bitmaps rather than sorted
+ * keys (0: automatic). It changes the speed, never the result. */
+ol_status ol_search_many_device(ol_ctx *ctx, const ol_doc *doc, const ol_patset *set, uint64_t max_hits,
+                                uint32_t heavy_min_hits, uint32_t *counts, uint64_t *total_hits, ol_hit *d_hits);
+
 /* ---- substring search that allocates nothing. No counterpart in the
  *      reference: an addition for callers that cannot call cudaMalloc, such as a
  *      serving process whose own allocator reserved the GPU's memory up front, or

@@ -10,8 +10,15 @@ from .gpu import (  # noqa: F401
     MAX_GPU_INPUT_LEN,
     MAX_PATTERN_LEN,
     MAX_TREE_DEPTH,
+    HIT_DTYPE,
+    MAX_DICT_PATTERNS,
+    MAX_PATTERNS,
+    MAX_SET_PATTERN_LEN,
+    MIN_SET_PATTERN_LEN,
     GpuDocument,
     GpuParser,
+    GpuPatternSet,
     GpuTree,
+    ManyResult,
     SearchResult,
 )

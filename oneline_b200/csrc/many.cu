@@ -1,0 +1,516 @@
+// Kernel (e): dictionary search. Every (pattern, offset) at which one of a set
+// of patterns (4..64 bytes, up to 65,536 of them) occurs, ordered by
+// (pattern, offset) like ManyPatterns::find_all_par
+// (crates/oneline-simd/src/search.rs:259-282). Replaces the reference's
+// window-filter kernels and host sort (crates/oneline-gpu/src/many.rs:391-646).
+//
+// The compiled set (runtime_many.cu) deduplicates the patterns and builds a
+// trie over the unique ones; its depth-4 nodes are reached through a hash
+// table keyed by a position's first four bytes, and a two-hash filter of those
+// keys (16 KiB) sits in shared memory, copied there once per block with a bulk
+// TMA copy (cp.async.bulk, no multicast).
+//
+// dict_match_kernel: persistent blocks walk 16 KiB tiles staged in shared
+// memory. Each warp takes 32 consecutive positions at a time (lane = position):
+// filter, table probe, then all lanes walk the trie one depth per iteration.
+// A unique pattern u of length d is met at depth d by every lane where it
+// occurs, so `__match_any_sync` on u at that depth groups exactly those lanes:
+//   * heavy patterns (chosen per search from a sample of the text) get one
+//     bitmap word per 32 positions, the group's lane mask, written without
+//     atomics through a per-warp staging area, sector by sector;
+//   * light patterns append (u << 32 | offset) keys with one warp-aggregated
+//     atomic per depth, and their counts with one atomic per group.
+// Then: popcounts of the bitmaps and a column scan give every heavy hit its
+// rank; a stable radix sort orders the light keys; a single-block pass gives
+// every pattern id its first output slot; the emit kernels write each hit
+// once per id that holds the same bytes (duplicates are reported once per id).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "ol_common.cuh"
+#include "ol_kernels.h"
+
+namespace ol {
+
+constexpr uint32_t DM_THREADS = 256;
+constexpr uint32_t DM_WARPS = DM_THREADS / 32;
+constexpr uint32_t DM_POS_PER_WARP = kDictTile / DM_WARPS;  // 2048
+constexpr uint32_t DM_STEPS = DM_POS_PER_WARP / 32;          // 64
+constexpr uint32_t DM_FLUSH = 8;                              // bitmap words staged per heavy pattern
+constexpr uint32_t DM_FILTER_WORDS = 1u << (kDictFilterBits - 5);
+constexpr uint32_t DM_TEXT_BYTES = kDictTile + kDictHalo;
+constexpr uint32_t kMbarSpins = 1u << 24;
+static_assert(DM_STEPS % DM_FLUSH == 0, "flush windows");
+static_assert(DM_TEXT_BYTES % 16 == 0, "16-byte staging");
+
+struct DictSmem {
+    uint32_t filter[DM_FILTER_WORDS];
+    alignas(16) uint8_t text[DM_TEXT_BYTES];
+    uint32_t stage[DM_WARPS][kDictMaxHeavy * DM_FLUSH];
+    alignas(8) unsigned long long bar;
+};
+
+// ---------------------------------------------------------------- TMA bulk --
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// Global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, unsigned long long *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kMbarSpins; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(ok)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// ------------------------------------------------------------ trie walk ----
+
+__device__ __forceinline__ uint32_t dict_child(const DictSet &s, const uint4 &nd, uint32_t b) {
+    const uint32_t n = nd.y;
+    if (n == 0) return NONE;
+    uint32_t e0 = nd.z & 0xFFu;
+    if (e0 == b) return nd.z >> 8;
+    if (n == 1 || b < e0) return NONE;
+    if (n == 2) return (nd.w & 0xFFu) == b ? nd.w >> 8 : NONE;
+    for (uint32_t i = 0; i < n - 1; i++) {
+        uint32_t e = __ldg(s.extra + nd.w + i);
+        uint32_t eb = e & 0xFFu;
+        if (eb == b) return e >> 8;
+        if (eb > b) break;
+    }
+    return NONE;
+}
+
+__device__ __forceinline__ uint32_t dict_probe(const DictSet &s, uint32_t key) {
+    const uint32_t mask = (1u << s.table_bits) - 1u;
+    uint32_t slot = dict_table_h(key, s.table_bits);
+    for (uint32_t i = 0; i <= s.max_probe; i++) {
+        uint2 e = __ldg(s.table + slot);
+        if (e.y == NONE) return NONE;
+        if (e.x == key) return e.y;
+        slot = (slot + 1) & mask;
+    }
+    return NONE;
+}
+
+// ------------------------------------------------------------- matching ----
+
+__global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a) {
+    extern __shared__ __align__(16) uint8_t dyn_smem[];
+    DictSmem &sm = *reinterpret_cast<DictSmem *>(dyn_smem);
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+
+    // The filter, once per block, by a bulk copy.
+    if (tid == 0) mbar_init(&sm.bar, 1);
+    __syncthreads();
+    if (tid == 0) {
+        mbar_expect_tx(&sm.bar, DM_FILTER_WORDS * 4);
+        bulk_copy_g2s(sm.filter, a.set.filter, DM_FILTER_WORDS * 4, &sm.bar);
+    }
+    bool ok = mbar_wait(&sm.bar, 0);
+    if (!__syncthreads_and(ok)) {
+        if (tid == 0) atomicOr(a.error, OL_DEVERR_TIMEOUT);
+        mbar_wait(&sm.bar, 0);  // let the copy land before the block exits
+        return;
+    }
+
+    const uint32_t n_work = (a.n_tiles + a.tile_stride - 1) / a.tile_stride;
+    const uint64_t N = a.text_len;
+    const uint32_t n_words = a.n_tiles * kDictWordsPerTile;
+    uint32_t *stage = sm.stage[warp];
+    const uint32_t H = a.n_heavy;
+
+    for (uint32_t k = blockIdx.x; k < n_work; k += gridDim.x) {
+        const uint32_t tile = k * a.tile_stride;
+        const uint64_t t0 = (uint64_t)tile * kDictTile;
+        __syncthreads();  // the previous tile's text is no longer read
+        for (uint32_t o = tid * 16; o < DM_TEXT_BYTES; o += DM_THREADS * 16)
+            *reinterpret_cast<uint4 *>(&sm.text[o]) = ld_stream16(a.text + t0 + o);
+        __syncthreads();
+        const uint32_t *tw = reinterpret_cast<const uint32_t *>(sm.text);
+
+        for (uint32_t s = 0; s < DM_STEPS; s++) {
+            if (!a.count_only && (s % DM_FLUSH) == 0) {
+                for (uint32_t f = lane; f < H * DM_FLUSH; f += 32) stage[f] = 0;
+                __syncwarp();
+            }
+            const uint32_t p = warp * DM_POS_PER_WARP + s * 32 + lane;  // tile-local position
+            const uint64_t pos = t0 + p;
+            uint32_t v = NONE;
+            if (pos + kDictMinLen <= N) {
+                const uint32_t key = __funnelshift_r(tw[p >> 2], tw[(p >> 2) + 1], (p & 3) * 8);
+                const uint32_t h1 = dict_filter_h1(key), h2 = dict_filter_h2(key);
+                if (((sm.filter[h1 >> 5] >> (h1 & 31)) & (sm.filter[h2 >> 5] >> (h2 & 31)) & 1u) != 0)
+                    v = dict_probe(a.set, key);
+            }
+            uint32_t d = kDictMinLen;
+            while (__any_sync(0xFFFFFFFFu, v != NONE)) {
+                uint4 nd = make_uint4(NONE, 0, 0, 0);
+                if (v != NONE) nd = __ldg(a.set.nodes + v);
+                const uint32_t u = nd.x;
+                const bool emit = u != NONE && pos + d <= N;
+                const uint32_t em = __ballot_sync(0xFFFFFFFFu, emit);
+                if (emit) {
+                    const uint32_t peers = __match_any_sync(em, u);
+                    const bool leader = (peers & lt) == 0;
+                    if (a.count_only) {
+                        if (leader) atomicAdd(a.counts + u, (uint32_t)__popc(peers));
+                    } else {
+                        const uint32_t hv = __ldg(a.heavy_of_u + u);
+                        const bool light = hv == 0xFFu;
+                        if (!light && leader) stage[hv * DM_FLUSH + (s % DM_FLUSH)] = peers;
+                        const uint32_t lm = __ballot_sync(em, light);
+                        if (light) {
+                            if (leader) atomicAdd(a.counts + u, (uint32_t)__popc(peers));
+                            const uint32_t first = __ffs(lm) - 1;
+                            uint32_t base = 0;
+                            if (lane == first) base = atomicAdd(a.light_n, (uint32_t)__popc(lm));
+                            base = __shfl_sync(lm, base, first);
+                            const uint32_t slot = base + __popc(lm & lt);
+                            if (slot < a.light_cap) a.light_keys[slot] = ((unsigned long long)u << 32) | (uint32_t)pos;
+                        }
+                    }
+                }
+                uint32_t nv = NONE;
+                if (v != NONE && d < kDictMaxLen && pos + d < N) nv = dict_child(a.set, nd, sm.text[p + d]);
+                v = nv;
+                d++;
+            }
+            if (!a.count_only && (s % DM_FLUSH) == DM_FLUSH - 1) {
+                __syncwarp();
+                // words [wbase, wbase + 8) of every heavy bitmap: 32-byte sectors
+                const uint32_t wbase = tile * kDictWordsPerTile + warp * (DM_POS_PER_WARP / 32) + (s - (DM_FLUSH - 1));
+                for (uint32_t f = lane; f < H * DM_FLUSH; f += 32)
+                    a.bitmap[(size_t)(f / DM_FLUSH) * n_words + wbase + (f % DM_FLUSH)] = stage[f];
+                __syncwarp();
+            }
+        }
+    }
+}
+
+cudaError_t launch_dict_match(const DictMatchArgs &a, int sm_count, cudaStream_t st) {
+    if (a.n_tiles == 0) return cudaSuccess;
+    const size_t smem = sizeof(DictSmem);
+    cudaError_t e = cudaFuncSetAttribute(dict_match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dict_match_kernel, DM_THREADS, smem);
+    if (e != cudaSuccess) return e;
+    const uint32_t n_work = (a.n_tiles + a.tile_stride - 1) / a.tile_stride;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(n_work, (uint64_t)std::max(per_sm, 1) * sm_count);
+    dict_match_kernel<<<grid, DM_THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ heavy ranks --
+
+constexpr uint32_t DH_THREADS = 256;
+constexpr uint32_t DH_WORDS_PER_THREAD = 16;
+constexpr uint32_t DH_WORDS = DH_THREADS * DH_WORDS_PER_THREAD;  // 4096 words per block
+
+uint32_t dict_heavy_blocks(uint32_t n_words) { return (n_words + DH_WORDS - 1) / DH_WORDS; }
+
+// Block sum / exclusive scan helpers for 256 threads.
+__device__ __forceinline__ uint32_t block_exclusive_256(uint32_t x, uint32_t *warp_sum, uint32_t *total) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if ((int)lane >= o) inc += t;
+    }
+    if (lane == 31) warp_sum[warp] = inc;
+    __syncthreads();
+    uint32_t before = 0, all = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < DH_THREADS / 32; w++) {
+        uint32_t ws = warp_sum[w];
+        before += w < warp ? ws : 0u;
+        all += ws;
+    }
+    __syncthreads();
+    if (total) *total = all;
+    return before + inc - x;
+}
+
+__global__ void __launch_bounds__(DH_THREADS) dict_heavy_count_kernel(const uint32_t *__restrict__ bitmap,
+                                                                       uint32_t n_words, uint32_t *counts,
+                                                                       uint32_t ld) {
+    __shared__ uint32_t warp_sum[DH_THREADS / 32];
+    const uint32_t h = blockIdx.y, b = blockIdx.x;
+    const uint32_t w0 = b * DH_WORDS + threadIdx.x * DH_WORDS_PER_THREAD;
+    const uint32_t *col = bitmap + (size_t)h * n_words;
+    uint32_t c = 0;
+    if (w0 < n_words) {  // n_words is a multiple of 512: a thread's 16 words are all in range
+#pragma unroll
+        for (uint32_t i = 0; i < DH_WORDS_PER_THREAD; i += 4) {
+            uint4 q = __ldg(reinterpret_cast<const uint4 *>(col + w0 + i));
+            c += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
+        }
+    }
+    uint32_t total;
+    block_exclusive_256(c, warp_sum, &total);
+    if (threadIdx.x == 0) counts[(size_t)h * ld + b] = total;
+}
+
+cudaError_t launch_dict_heavy_count(const uint32_t *bitmap, uint32_t n_words, uint32_t n_heavy, uint32_t *counts,
+                                    uint32_t ld, cudaStream_t st) {
+    if (n_heavy == 0 || n_words == 0) return cudaSuccess;
+    dim3 grid(dict_heavy_blocks(n_words), n_heavy);
+    dict_heavy_count_kernel<<<grid, DH_THREADS, 0, st>>>(bitmap, n_words, counts, ld);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------- light-key radix sort --
+
+constexpr uint32_t DS_THREADS = 256;
+constexpr uint32_t DS_WARPS = DS_THREADS / 32;
+constexpr uint32_t DS_PER_LANE = kDictSortChunk / 32;
+
+uint32_t dict_sort_chunks(uint32_t n) { return (n + kDictSortChunk - 1) / kDictSortChunk; }
+
+// Per-warp digit histograms: chunk c (one warp) holds keys [512c, 512c + 512).
+__global__ void __launch_bounds__(DS_THREADS) dict_sort_hist_kernel(const unsigned long long *__restrict__ keys,
+                                                                     uint32_t n, uint32_t shift, uint32_t *hist,
+                                                                     uint32_t ld, uint32_t chunks) {
+    __shared__ uint32_t sh[DS_WARPS][256];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t c = blockIdx.x * DS_WARPS + warp;
+    for (uint32_t d = lane; d < 256; d += 32) sh[warp][d] = 0;
+    __syncwarp();
+    if (c < chunks) {
+#pragma unroll 4
+        for (uint32_t i = 0; i < DS_PER_LANE; i++) {
+            uint32_t idx = c * kDictSortChunk + i * 32 + lane;
+            if (idx < n) atomicAdd(&sh[warp][(uint32_t)(keys[idx] >> shift) & 255u], 1u);
+        }
+        __syncwarp();
+        for (uint32_t d = lane; d < 256; d += 32) hist[(size_t)d * ld + c] = sh[warp][d];
+    }
+}
+
+// Stable scatter: each warp walks its chunk in order, 32 keys at a time; lanes
+// with the same digit take consecutive slots in lane order.
+__global__ void __launch_bounds__(DS_THREADS) dict_sort_scatter_kernel(const unsigned long long *__restrict__ in,
+                                                                        unsigned long long *__restrict__ out,
+                                                                        uint32_t n, uint32_t shift,
+                                                                        const uint32_t *__restrict__ base,
+                                                                        const uint32_t *__restrict__ totals,
+                                                                        uint32_t ld, uint32_t chunks) {
+    __shared__ uint32_t start[256];
+    __shared__ uint32_t warp_sum[DS_WARPS];
+    __shared__ uint32_t cursor[DS_WARPS][256];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // digit starts: exclusive scan of the 256 digit totals
+    start[tid] = block_exclusive_256(totals[tid], warp_sum, nullptr);
+    __syncthreads();
+    const uint32_t c = blockIdx.x * DS_WARPS + warp;
+    if (c >= chunks) return;
+    for (uint32_t d = lane; d < 256; d += 32) cursor[warp][d] = start[d] + base[(size_t)d * ld + c];
+    __syncwarp();
+    const uint32_t lt = (1u << lane) - 1u;
+    for (uint32_t i = 0; i < DS_PER_LANE; i++) {
+        const uint32_t idx = c * kDictSortChunk + i * 32 + lane;
+        const bool valid = idx < n;
+        const uint32_t vm = __ballot_sync(0xFFFFFFFFu, valid);
+        if (!vm) break;
+        unsigned long long key = 0;
+        uint32_t d = 0, peers = 0;
+        if (valid) {
+            key = in[idx];
+            d = (uint32_t)(key >> shift) & 255u;
+            peers = __match_any_sync(vm, d);
+            out[cursor[warp][d] + __popc(peers & lt)] = key;
+        }
+        __syncwarp();
+        if (valid && (peers & lt) == 0) cursor[warp][d] += __popc(peers);
+        __syncwarp();
+    }
+}
+
+cudaError_t launch_dict_sort(unsigned long long *keys, unsigned long long *tmp, uint32_t n, uint32_t key_bits,
+                             uint32_t *hist, uint32_t *totals, cudaStream_t st) {
+    if (n < 2) return cudaSuccess;
+    const uint32_t chunks = dict_sort_chunks(n);
+    const uint32_t ld = scan_ld(chunks);
+    uint32_t *counts = hist, *bases = hist + (size_t)256 * ld;
+    const uint32_t blocks = (chunks + DS_WARPS - 1) / DS_WARPS;
+    unsigned long long *src = keys, *dst = tmp;
+    uint32_t passes = (key_bits + 7) / 8;
+    passes += passes & 1;  // an even number of passes leaves the result in keys
+    for (uint32_t p = 0; p < passes; p++) {
+        const uint32_t shift = 8 * p;
+        dict_sort_hist_kernel<<<blocks, DS_THREADS, 0, st>>>(src, n, shift, counts, ld, chunks);
+        cudaError_t e = launch_scan_columns(counts, bases, totals, chunks, 256, ld, st);
+        if (e != cudaSuccess) return e;
+        dict_sort_scatter_kernel<<<blocks, DS_THREADS, 0, st>>>(src, dst, n, shift, bases, totals, ld, chunks);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        unsigned long long *t = src;
+        src = dst;
+        dst = t;
+    }
+    return cudaSuccess;
+}
+
+// ------------------------------------------------------------------ ids ----
+
+constexpr uint32_t DI_THREADS = 1024;
+
+// One block: per id its count and first output slot (u64 exclusive scan in id
+// order), the total, and per unique pattern the start of its light keys.
+__global__ void __launch_bounds__(DI_THREADS) dict_ids_kernel(DictEmitArgs a) {
+    __shared__ unsigned long long wsum64[DI_THREADS / 32];
+    __shared__ uint32_t wsum32[DI_THREADS / 32];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    auto count_of_u = [&](uint32_t u) -> uint32_t {
+        uint32_t h = a.heavy_of_u[u];
+        return h == 0xFFu ? a.light_count[u] : a.heavy_totals[h];
+    };
+    // ids
+    {
+        const uint32_t per = (a.n_ids + DI_THREADS - 1) / DI_THREADS;
+        const uint32_t lo = min(a.n_ids, tid * per), hi = min(a.n_ids, lo + per);
+        unsigned long long sum = 0;
+        for (uint32_t i = lo; i < hi; i++) sum += count_of_u(a.u_of_id[i]);
+        unsigned long long inc = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if ((int)lane >= o) inc += t;
+        }
+        if (lane == 31) wsum64[warp] = inc;
+        __syncthreads();
+        unsigned long long before = 0, all = 0;
+        for (uint32_t w = 0; w < DI_THREADS / 32; w++) {
+            before += w < warp ? wsum64[w] : 0ull;
+            all += wsum64[w];
+        }
+        unsigned long long run = before + inc - sum;
+        for (uint32_t i = lo; i < hi; i++) {
+            uint32_t c = count_of_u(a.u_of_id[i]);
+            a.id_counts[i] = c;
+            a.id_base[i] = run;
+            run += c;
+        }
+        if (tid == 0) *a.total = all;
+    }
+    __syncthreads();
+    // light key starts per unique pattern
+    {
+        const uint32_t per = (a.n_u + DI_THREADS - 1) / DI_THREADS;
+        const uint32_t lo = min(a.n_u, tid * per), hi = min(a.n_u, lo + per);
+        uint32_t sum = 0;
+        for (uint32_t u = lo; u < hi; u++) sum += a.heavy_of_u[u] == 0xFFu ? a.light_count[u] : 0u;
+        uint32_t inc = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if ((int)lane >= o) inc += t;
+        }
+        if (lane == 31) wsum32[warp] = inc;
+        __syncthreads();
+        uint32_t before = 0;
+        for (uint32_t w = 0; w < warp; w++) before += wsum32[w];
+        uint32_t run = before + inc - sum;
+        for (uint32_t u = lo; u < hi; u++) {
+            a.light_base[u] = run;
+            run += a.heavy_of_u[u] == 0xFFu ? a.light_count[u] : 0u;
+        }
+    }
+}
+
+cudaError_t launch_dict_ids(const DictEmitArgs &a, cudaStream_t st) {
+    dict_ids_kernel<<<1, DI_THREADS, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------- emit ----
+
+// Heavy hits: block (b, h) expands words [4096b, 4096b + 4096) of bitmap h;
+// thread t owns 16 consecutive words, its first rank from a block scan.
+__global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArgs a) {
+    __shared__ uint32_t warp_sum[DH_THREADS / 32];
+    const uint32_t h = blockIdx.y, b = blockIdx.x;
+    const uint32_t w0 = b * DH_WORDS + threadIdx.x * DH_WORDS_PER_THREAD;
+    const uint32_t *col = a.bitmap + (size_t)h * a.n_words;
+    uint32_t c = 0;
+    if (w0 < a.n_words) {
+#pragma unroll
+        for (uint32_t i = 0; i < DH_WORDS_PER_THREAD; i += 4) {
+            uint4 q = __ldg(reinterpret_cast<const uint4 *>(col + w0 + i));
+            c += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
+        }
+    }
+    uint32_t rank = a.heavy_bases[(size_t)h * a.ld + b] + block_exclusive_256(c, warp_sum, nullptr);
+    if (c == 0) return;
+    const uint32_t u = a.heavy_u[h];
+    const uint32_t d0 = a.dup_start[u], d1 = a.dup_start[u + 1];
+    for (uint32_t i = 0; i < DH_WORDS_PER_THREAD; i++) {
+        uint32_t bits = __ldg(col + w0 + i);  // again: the words were just read
+        while (bits) {
+            const uint32_t bit = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const uint32_t off = (w0 + i) * 32 + bit;
+            for (uint32_t d = d0; d < d1; d++) {
+                const uint32_t id = a.dup_ids[d];
+                const unsigned long long slot = a.id_base[id] + rank;
+                if (slot < a.max_hits) a.hits[slot] = make_uint2(id, off);
+            }
+            rank++;
+        }
+    }
+}
+
+__global__ void dict_emit_light_kernel(DictEmitArgs a) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.light_n) return;
+    const unsigned long long key = a.light_keys[k];
+    const uint32_t u = (uint32_t)(key >> 32), off = (uint32_t)key;
+    const uint32_t rank = k - a.light_base[u];
+    const uint32_t d0 = a.dup_start[u], d1 = a.dup_start[u + 1];
+    for (uint32_t d = d0; d < d1; d++) {
+        const uint32_t id = a.dup_ids[d];
+        const unsigned long long slot = a.id_base[id] + rank;
+        if (slot < a.max_hits) a.hits[slot] = make_uint2(id, off);
+    }
+}
+
+cudaError_t launch_dict_emit(const DictEmitArgs &a, cudaStream_t st) {
+    if (a.max_hits == 0) return cudaSuccess;
+    if (a.n_heavy && a.n_words) {
+        dim3 grid(dict_heavy_blocks(a.n_words), a.n_heavy);
+        dict_emit_heavy_kernel<<<grid, DH_THREADS, 0, st>>>(a);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (a.light_n) {
+        dict_emit_light_kernel<<<(a.light_n + 255) / 256, 256, 0, st>>>(a);
+        return cudaGetLastError();
+    }
+    return cudaSuccess;
+}
+
+}  // namespace ol

@@ -99,4 +99,87 @@ struct SearchArgs {
 
 cudaError_t launch_search(const SearchArgs &a, cudaStream_t st);
 
+// ------------------------------------------------------------ dictionary --
+
+constexpr uint32_t kDictTile = 16384;         // text bytes per tile (the parse tile: same padding)
+constexpr uint32_t kDictHalo = 80;            // staged past the tile: > longest pattern, 16-byte multiple
+constexpr uint32_t kDictMinLen = 4;           // the filter keys on a pattern's first 4 bytes
+constexpr uint32_t kDictMaxLen = 64;
+constexpr uint32_t kDictMaxHeavy = 32;        // patterns whose hits go to bitmaps in one search
+constexpr uint32_t kDictFilterBits = 17;      // 2^17-bit two-hash filter (16 KiB of shared memory)
+constexpr uint32_t kDictWordsPerTile = kDictTile / 32;
+constexpr uint32_t kDictSortChunk = 512;      // keys per warp in the light-hit radix sort
+
+// Filter and table hashes of a pattern's first four bytes (little-endian u32);
+// the host compiler uses the same functions.
+__host__ __device__ inline uint32_t dict_filter_h1(uint32_t w) { return (w * 0x85EBCA77u) >> (32 - kDictFilterBits); }
+__host__ __device__ inline uint32_t dict_filter_h2(uint32_t w) { return (w * 0xC2B2AE3Du) >> (32 - kDictFilterBits); }
+__host__ __device__ inline uint32_t dict_table_h(uint32_t w, uint32_t bits) { return (w * 0x9E3779B1u) >> (32 - bits); }
+
+// Device view of a compiled pattern set. Patterns are deduplicated ("unique
+// patterns" u); a trie over them gives, for a text position whose first four
+// bytes match some pattern's, every unique pattern starting there.
+struct DictSet {
+    const uint32_t *filter;  // 2^kDictFilterBits bits
+    const uint2 *table;      // open addressing: {first 4 bytes, trie node at depth 4}; empty: .y == NONE
+    uint32_t table_bits;
+    uint32_t max_probe;      // longest probe distance of any key
+    const uint4 *nodes;      // {unique pattern ending here or NONE, edge count, edge 0, edge 1 | extra start}
+    const uint32_t *extra;   // edges 1.. of nodes with more than two; edge = (child << 8) | byte, sorted by byte
+    uint32_t n_u;
+};
+
+struct DictMatchArgs {
+    DictSet set;
+    const uint8_t *text;     // padded like every resident text
+    uint64_t text_len;
+    uint32_t n_tiles;
+    uint32_t tile_stride;    // tiles 0, s, 2s, ... (count mode samples)
+    uint32_t count_only;     // 1: counts[u] += every hit; 0: heavy bitmaps + light keys
+    uint32_t *counts;        // per unique pattern (count mode: all hits; else light hits)
+    const uint8_t *heavy_of_u;  // heavy index or 0xFF
+    uint32_t n_heavy;
+    uint32_t *bitmap;        // [n_heavy][n_tiles * kDictWordsPerTile]
+    unsigned long long *light_keys;  // (u << 32) | offset, unordered
+    uint32_t light_cap;
+    uint32_t *light_n;
+    uint32_t *error;
+};
+
+cudaError_t launch_dict_match(const DictMatchArgs &a, int sm_count, cudaStream_t st);
+// Per (4096-word block, heavy pattern) popcounts, [n_heavy][ld] column-major.
+cudaError_t launch_dict_heavy_count(const uint32_t *bitmap, uint32_t n_words, uint32_t n_heavy, uint32_t *counts,
+                                    uint32_t ld, cudaStream_t st);
+uint32_t dict_heavy_blocks(uint32_t n_words);
+// Stable LSD radix sort of n 64-bit keys on bits [0, key_bits), 8 per pass;
+// the result ends in keys (tmp is the other buffer); hist needs
+// 2 * 256 * scan_ld(chunks) words and digit totals 256 words.
+cudaError_t launch_dict_sort(unsigned long long *keys, unsigned long long *tmp, uint32_t n, uint32_t key_bits,
+                             uint32_t *hist, uint32_t *totals, cudaStream_t st);
+uint32_t dict_sort_chunks(uint32_t n);
+
+struct DictEmitArgs {
+    uint32_t n_ids, n_u, n_heavy, n_words;
+    const uint32_t *u_of_id;
+    const uint32_t *dup_start;   // [n_u + 1]
+    const uint32_t *dup_ids;     // ids grouped by unique pattern, ascending
+    const uint8_t *heavy_of_u;
+    const uint32_t *heavy_u;     // [n_heavy]
+    const uint32_t *heavy_totals;
+    const uint32_t *heavy_bases; // [n_heavy][ld]
+    uint32_t ld;
+    const uint32_t *bitmap;
+    const uint32_t *light_count; // [n_u]
+    uint32_t *light_base;        // [n_u] (written by the id pass)
+    const unsigned long long *light_keys;  // sorted
+    uint32_t light_n;
+    uint32_t *id_counts;         // [n_ids]
+    unsigned long long *id_base; // [n_ids]
+    unsigned long long *total;
+    uint2 *hits;                 // {pattern, offset}
+    unsigned long long max_hits;
+};
+cudaError_t launch_dict_ids(const DictEmitArgs &a, cudaStream_t st);
+cudaError_t launch_dict_emit(const DictEmitArgs &a, cudaStream_t st);
+
 }  // namespace ol

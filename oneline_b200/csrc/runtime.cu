@@ -132,6 +132,10 @@ extern "C" void ol_ctx_destroy(ol_ctx *ctx) {
     ctx->scratch_c.release(ctx->stream);
     ctx->search_out.release(ctx->stream);
     ctx->pattern_dev.release(ctx->stream);
+    ctx->dict_small.release(ctx->stream);
+    ctx->dict_bitmap.release(ctx->stream);
+    ctx->dict_keys.release(ctx->stream);
+    ctx->dict_hits.release(ctx->stream);
     if (ctx->counters) cudaFreeAsync(ctx->counters, ctx->stream);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->host_counters) cudaFreeHost(ctx->host_counters);

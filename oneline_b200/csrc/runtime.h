@@ -46,6 +46,10 @@ struct ol_ctx {
     ol::DevBuf scratch_c;  // nodes and other per-call outputs
     ol::DevBuf search_out;
     ol::DevBuf pattern_dev;
+    ol::DevBuf dict_small;   // dictionary search: per-pattern counts, ranks, slots
+    ol::DevBuf dict_bitmap;  // heavy-pattern bitmaps
+    ol::DevBuf dict_keys;    // light-hit keys and the sort's second buffer
+    ol::DevBuf dict_hits;    // hits of the blocking search before the download
     ol::CtxCounters *counters = nullptr;
     ol::CtxCounters *host_counters = nullptr;  // pinned
     uint8_t *pat_host = nullptr;  // pinned staging for pattern bytes

@@ -7,6 +7,8 @@ Method names, argument meaning and error behaviour follow the reference:
 * ``GpuParser.build_tree`` / ``build_tree_reusing`` / ``download_links`` / ``GpuTree``
                                                         tree.rs:34-67, 278-290
 * ``GpuParser.search_document`` / ``search_raw`` / ``SearchResult``  search.rs:12-140
+* ``GpuParser.compile_patterns`` / ``search_many`` / ``GpuPatternSet`` / ``ManyResult``
+                                                        many.rs:14-18, 76-94, 139-176, 391-399
 * limits ``MAX_PATTERN_LEN``, ``MAX_TREE_DEPTH``, ``MAX_GPU_INPUT_LEN``  lib.rs:66, tree.rs:12, util.rs:8
 
 Errors are raised as ``OnelineError`` (the reference returns ``anyhow::Error``);
@@ -26,6 +28,11 @@ from ._lib import OnelineError, check
 from .core import NODE_DTYPE, NONE, FlatTree, TreeLinks
 
 MAX_PATTERN_LEN = 64
+MAX_PATTERNS = 2048           # many.rs:14 (drop-in set size)
+MIN_SET_PATTERN_LEN = 4       # many.rs:17
+MAX_SET_PATTERN_LEN = 64      # many.rs:18
+MAX_DICT_PATTERNS = 65536     # this engine's set size limit
+HIT_DTYPE = np.dtype([("pattern", "<u4"), ("offset", "<u4")])  # ManyHit (many.rs:76-82)
 MAX_TREE_DEPTH = 32
 MAX_GPU_INPUT_LEN = 0xFFFFFFFF - 3
 TREE_STRICT_DEPTH = 1
@@ -142,6 +149,54 @@ class GpuTree:
     def free(self) -> None:
         if self._h and self._parser._ctx:
             _lib.load().ol_tree_free(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+@dataclass
+class ManyResult:
+    """Result of a dictionary search (many.rs:84-94). ``hits`` is a structured
+    array (``pattern``, ``offset``) sorted by (pattern, offset); when there are more
+    than ``max_hits`` it holds the first ``max_hits`` of that order."""
+
+    counts: np.ndarray
+    total_hits: int
+    hits: np.ndarray = field(default_factory=lambda: np.zeros(0, HIT_DTYPE))
+
+
+class GpuPatternSet:
+    """A compiled dictionary (many.rs:116-147)."""
+
+    def __init__(self, parser: "GpuParser", handle: int, n: int):
+        self._parser = parser
+        self._h = handle
+        self._n = n
+        parser._children.add(self)
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def __len__(self) -> int:
+        return self._n
+
+    def len(self) -> int:
+        return self._n
+
+    def is_empty(self) -> bool:
+        return self._n == 0
+
+    def unique(self) -> int:
+        return int(_lib.load().ol_patset_unique(self._h))
+
+    def free(self) -> None:
+        if self._h and self._parser._ctx:
+            _lib.load().ol_patset_free(self._h)
         self._h = None
 
     def __del__(self):
@@ -334,3 +389,50 @@ class GpuParser:
                                         ctypes.byref(total), out.ctypes.data), self._ctx)
         k = min(total.value, max_matches)
         return SearchResult(total.value, out[:k].copy())
+
+    def compile_patterns(self, doc: GpuDocument | None, patterns, *,
+                         max_patterns: int | None = MAX_PATTERNS) -> GpuPatternSet:
+        """Compiles a dictionary (many.rs:158-176): 1..=2048 patterns of 4..=64 bytes, like
+        the reference; ``max_patterns=None`` allows up to 65,536."""
+        pats = [p.encode("utf-8") if isinstance(p, str) else bytes(p) for p in patterns]
+        limit = MAX_DICT_PATTERNS if max_patterns is None else min(max_patterns, MAX_DICT_PATTERNS)
+        if not 1 <= len(pats) <= limit:
+            raise OnelineError(3, f"pattern count {len(pats)} is outside 1..={limit}")
+        for i, p in enumerate(pats):
+            if not MIN_SET_PATTERN_LEN <= len(p) <= MAX_SET_PATTERN_LEN:
+                raise OnelineError(3, f"pattern {i} has {len(p)} bytes; set patterns need "
+                                      f"{MIN_SET_PATTERN_LEN}..={MAX_SET_PATTERN_LEN}")
+        bufs = [np.frombuffer(p, np.uint8) for p in pats]
+        P = (ctypes.c_void_p * len(pats))(*[b.ctypes.data for b in bufs])
+        lens = np.array([len(p) for p in pats], np.uint32)
+        h = ctypes.c_void_p()
+        check(_lib.load().ol_patset_compile(self._ctx, doc.handle if doc is not None else None, P,
+                                            lens.ctypes.data, len(pats), ctypes.byref(h)), self._ctx)
+        return GpuPatternSet(self, h.value, len(pats))
+
+    def search_many(self, doc: GpuDocument, pattern_set: GpuPatternSet, max_hits: int) -> ManyResult:
+        """Every (pattern, offset) of the set in ``doc`` (many.rs:391-399): counts per
+        pattern, the total, and up to ``max_hits`` hits in (pattern, offset) order."""
+        if max_hits < 0:
+            raise OnelineError(1, "max_hits must not be negative")
+        n = len(pattern_set)
+        counts = np.zeros(n, np.uint32)
+        total = ctypes.c_uint64()
+        hits = np.zeros(max(int(max_hits), 1), HIT_DTYPE)
+        check(_lib.load().ol_search_many(self._ctx, doc.handle, pattern_set.handle, int(max_hits),
+                                         counts.ctypes.data, ctypes.byref(total), hits.ctypes.data), self._ctx)
+        k = min(int(total.value), int(max_hits))
+        return ManyResult(counts, int(total.value), hits[:k].copy())
+
+    def search_many_device(self, doc: GpuDocument, pattern_set: GpuPatternSet, d_hits: int, max_hits: int, *,
+                           heavy_min_hits: int = 0) -> tuple[np.ndarray, int]:
+        """``search_many`` with the hits left in device memory at ``d_hits`` (room for
+        ``max_hits``); returns (counts, total_hits). ``heavy_min_hits`` tunes how hits
+        are collected (0: automatic) and never changes the result."""
+        n = len(pattern_set)
+        counts = np.zeros(n, np.uint32)
+        total = ctypes.c_uint64()
+        check(_lib.load().ol_search_many_device(self._ctx, doc.handle, pattern_set.handle, int(max_hits),
+                                                int(heavy_min_hits), counts.ctypes.data, ctypes.byref(total),
+                                                d_hits), self._ctx)
+        return counts, int(total.value)

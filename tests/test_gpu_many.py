@@ -1,0 +1,125 @@
+"""Dictionary search on the GPU vs the oracle: counts, total and every
+(pattern, offset) hit, in (pattern, offset) order, duplicates once per id.
+
+Mirrors crates/oneline-gpu/src/tests.rs:754-907 (assert_many_matches_cpu with
+duplicate, nested and colliding patterns) against ManyPatterns semantics
+(crates/oneline-simd/src/search.rs:259-312).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from oneline_b200 import HIT_DTYPE, OnelineError
+from oneline_b200 import datagen
+from tests.conftest import to_bytes
+
+pytestmark = pytest.mark.gpu
+
+
+def want_many(text: bytes, pats, fast=False):
+    if fast:
+        counts, hp, ho, total = oracle.CpuBaseline(threads=8).many(pats).find_all_par(text)
+    else:
+        counts, hp, ho = oracle.find_many(text, pats)
+        total = len(hp)
+    return counts.astype(np.uint64), int(total), hp, ho
+
+
+def assert_many(parser, text: bytes, pats, max_hits=None, fast=False, what=""):
+    counts, total, hp, ho = want_many(text, pats, fast)
+    doc = parser.upload(text)
+    ps = parser.compile_patterns(doc, pats, max_patterns=None)
+    cap = total if max_hits is None else max_hits
+    r = parser.search_many(doc, ps, cap)
+    assert r.total_hits == total, what
+    assert np.array_equal(r.counts.astype(np.uint64), counts), what
+    k = min(cap, total)
+    assert np.array_equal(r.hits["pattern"], hp[:k]), what
+    assert np.array_equal(r.hits["offset"], ho[:k]), what
+    return r
+
+
+def assert_many_device(parser, text: bytes, pats, heavy_min_hits, fast=False, what=""):
+    import torch
+
+    counts, total, hp, ho = want_many(text, pats, fast)
+    doc = parser.upload(text)
+    ps = parser.compile_patterns(doc, pats, max_patterns=None)
+    buf = torch.full((2 * max(total, 1),), -1, dtype=torch.int32, device="cuda")
+    c, t = parser.search_many_device(doc, ps, buf.data_ptr(), total, heavy_min_hits=heavy_min_hits)
+    hits = buf.cpu().numpy().view(HIT_DTYPE)[:total]
+    assert t == total and np.array_equal(c.astype(np.uint64), counts), what
+    assert np.array_equal(hits["pattern"], hp) and np.array_equal(hits["offset"], ho), what
+
+
+def test_reference_cases(parser, golden):
+    for key in ("many_nested", "many_whole_text", "many_longer_than_text"):
+        case = golden["edge_inputs"][key]
+        assert_many(parser, to_bytes(case["text"]), [to_bytes(p) for p in case["patterns"]], what=key)
+
+
+@pytest.mark.parametrize("profile", datagen.ALL_PROFILES)
+def test_generated_documents(parser, profile):
+    text = datagen.generate(profile, 2 << 20, 31)
+    pats = datagen.patterns_dictionary(np.frombuffer(text, np.uint8), 31, n=400)
+    pats += [b"||||", b"||||", b"| | ", b"\n|| ", text[:4], text[-4:], text[-64:], b"\x00\x00\x00\x00"]
+    assert_many(parser, text, pats, what=f"profile {profile}")
+
+
+def test_heavy_bitmaps_and_light_keys_give_the_same_hits(parser):
+    """Both ways of collecting hits, and the split between them, leave the result unchanged."""
+    text = datagen.corpus(3 << 20, 8).tobytes()
+    pats = datagen.patterns_dictionary(np.frombuffer(text, np.uint8), 8, n=500)
+    for heavy_min_hits in (1, 50, 1 << 30):
+        assert_many_device(parser, text, pats, heavy_min_hits, what=f"heavy >= {heavy_min_hits}")
+
+
+def test_benchmark_dictionary(parser):
+    """10,000 patterns (4..64 B, 60% sampled from the text) on the benchmark generator."""
+    text = datagen.corpus(4 << 20, 2).tobytes()
+    pats = datagen.patterns_dictionary(np.frombuffer(text, np.uint8), 2, n=10_000)
+    r = assert_many(parser, text, pats, fast=True)
+    assert r.total_hits > 10 * len(text) // 16
+    assert_many(parser, text, pats, max_hits=123_457, fast=True, what="truncated")
+
+
+def test_tile_edges_text_end_and_duplicates(parser):
+    text = bytearray(datagen.corpus(1 << 20, 4).tobytes())
+    pats = []
+    for edge in (16384, 2 * 16384, 5 * 16384, len(text)):
+        for n in (4, 5, 17, 63, 64):
+            for back in (0, 1, 3, n - 1, n):
+                at = edge - back
+                if 0 <= at and at + n <= len(text):
+                    pats.append(bytes(text[at: at + n]))
+    pats += pats[:7]  # duplicates: each id reports every occurrence
+    text[-1:] = b"\x00"
+    pats += [bytes(text[-3:]) + b"\x00", b"\x00" * 4]  # would only match the zero padding past the end
+    assert_many(parser, bytes(text), pats)
+
+
+def test_truncation_and_count_only(parser):
+    text = datagen.generate(datagen.MIXED, 1 << 20, 6)
+    pats = [b"||||", b"| | ", b"lorem", b"ipsum dolor", b"\n|||"]
+    r = assert_many(parser, text, pats, max_hits=1000)
+    assert len(r.hits) == 1000
+    doc = parser.upload(text)
+    r0 = parser.search_many(doc, parser.compile_patterns(doc, pats), 0)
+    assert r0.hits.size == 0 and r0.total_hits == r.total_hits
+
+
+def test_limits_errors_and_empty_document(parser):
+    doc = parser.upload(b"abcdefgh")
+    for bad in ([], [b"abc"], [b"a" * 65], [b"abcd"] * 2049):
+        with pytest.raises(OnelineError):
+            parser.compile_patterns(doc, bad)
+    parser.compile_patterns(doc, [b"abcd"] * 2049, max_patterns=None)
+    ps = parser.compile_patterns(doc, [b"abcd", b"efgh"])
+    assert len(ps) == 2 and not ps.is_empty()
+    r = parser.search_many(doc, ps, 10)
+    assert r.counts.tolist() == [1, 1] and r.hits.tolist() == [(0, 0), (1, 4)]
+    empty = parser.upload(b"")
+    r = parser.search_many(empty, ps, 10)
+    assert r.total_hits == 0 and r.counts.tolist() == [0, 0]
+    r = parser.search_many(parser.upload(b"abc"), ps, 10)
+    assert r.total_hits == 0
