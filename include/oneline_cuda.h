@@ -153,6 +153,24 @@ ol_status ol_search_multi(ol_ctx *ctx, const ol_doc *doc, const uint8_t *const *
 ol_status ol_search_multi_async(ol_ctx *ctx, const ol_doc *doc, const uint8_t *const *patterns, const uint32_t *lens,
                                 uint32_t n, const uint32_t *max_matches, uint32_t *d_totals, uint32_t *const *d_outs);
 
+/* ---- node queries: GpuParser::query_document / query_subtree / query_raw /
+ *      query (crates/oneline-gpu/src/document.rs:94-127, tree.rs:292-313,
+ *      query.rs:228-329). kind: a NodeKind code, 0 for any (the reference maps
+ *      None to 0, so Blank cannot be asked for either); depth: OL_ANY_DEPTH for
+ *      any. *total receives the number of matching lines, out the first
+ *      min(total, max_matches) of them in ascending order (the reference returns
+ *      an arbitrary subset when truncated). query_subtree considers lines
+ *      [root, subtree_end[root]). */
+#define OL_ANY_DEPTH 0xFFFFFFFFu
+ol_status ol_query_document(ol_ctx *ctx, const ol_doc *doc, uint32_t kind, uint32_t depth, uint32_t max_matches,
+                            uint32_t *total, uint32_t *out);
+ol_status ol_query_subtree(ol_ctx *ctx, const ol_doc *doc, const ol_tree *tree, uint64_t root, uint32_t kind,
+                           uint32_t depth, uint32_t max_matches, uint32_t *total, uint32_t *out);
+ol_status ol_query_raw(ol_ctx *ctx, const uint8_t *text, uint64_t len, uint32_t kind, uint32_t depth,
+                       uint32_t max_matches, uint32_t *total, uint32_t *out);
+ol_status ol_query(ol_ctx *ctx, const uint8_t *text, uint64_t len, const uint32_t *offsets, uint64_t n_lines,
+                   uint32_t kind, uint32_t depth, uint32_t max_matches, uint32_t *total, uint32_t *out);
+
 /* ---- dictionary search: GpuParser::compile_patterns / search_many,
  *      GpuPatternSet::{len, is_empty} (crates/oneline-gpu/src/many.rs:139-176,
  *      391-399). A set holds 1..OL_MAX_DICT_PATTERNS patterns of

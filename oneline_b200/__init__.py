@@ -20,5 +20,6 @@ from .gpu import (  # noqa: F401
     GpuPatternSet,
     GpuTree,
     ManyResult,
+    QueryResult,
     SearchResult,
 )

@@ -60,13 +60,17 @@ SIGNATURES: dict[str, tuple] = {
     "ol_search_async": (_S, [_P, _P, _U8P, _U32, _U32, _P, _P]),
     "ol_search_multi": (_S, [_P, _P, _P, _P, _U32, _P, _P, _P]),
     "ol_search_multi_async": (_S, [_P, _P, _P, _P, _U32, _P, _P, _P]),
+    "ol_query_document": (_S, [_P, _P, _U32, _U32, _U32, _U32P, _P]),
+    "ol_query_subtree": (_S, [_P, _P, _P, _U64, _U32, _U32, _U32, _U32P, _P]),
+    "ol_query_raw": (_S, [_P, _U8P, _U64, _U32, _U32, _U32, _U32P, _P]),
+    "ol_query": (_S, [_P, _U8P, _U64, _P, _U64, _U32, _U32, _U32, _U32P, _P]),
     "ol_patset_compile": (_S, [_P, _P, _P, _P, _U32, _PP]),
     "ol_patset_free": (None, [_P]),
     "ol_patset_len": (_U32, [_P]),
     "ol_patset_unique": (_U32, [_P]),
     "ol_search_many": (_S, [_P, _P, _P, _U64, _P, _U64P, _P]),
     "ol_search_many_device": (_S, [_P, _P, _P, _U64, _U32, _P, _U64P, _P]),
-    "ol_search_noalloc":(_S, [_U8P, _U64, _U64, _U8P, _U32, _U32, _P, _P, _P, ctypes.c_char_p, _U32]),
+    "ol_search_noalloc": (_S, [_U8P, _U64, _U64, _U8P, _U32, _U32, _P, _P, _P, ctypes.c_char_p, _U32]),
 }
 
 _lib = None

@@ -99,6 +99,28 @@ struct SearchArgs {
 
 cudaError_t launch_search(const SearchArgs &a, cudaStream_t st);
 
+// ---------------------------------------------------------------- query --
+
+struct QueryArgs {
+    const uint8_t *kinds;    // resident document (kinds, depth8, text, offsets) ...
+    const uint8_t *depth8;
+    const uint8_t *text;
+    const uint32_t *offsets;
+    uint64_t text_len;
+    const FlatNode *nodes;   // ... or materialised nodes (then the four above are unused)
+    uint32_t lines;          // lines in the document
+    uint32_t lo, hi;         // range [lo, hi) of lines considered
+    uint32_t target_kind;    // 0: any
+    uint32_t target_depth;   // NONE: any
+    uint32_t *counts;        // per block of 4096 lines, 16-byte aligned
+    uint32_t *bases;         // same size, 16-byte aligned
+    uint32_t *total;         // device
+    uint32_t *out;           // ascending line indices, first max_out of them
+    uint32_t max_out;
+};
+uint32_t query_blocks(uint32_t lines);
+cudaError_t launch_query(const QueryArgs &a, cudaStream_t st);
+
 // ------------------------------------------------------------ dictionary --
 
 constexpr uint32_t kDictTile = 16384;         // text bytes per tile (the parse tile: same padding)

@@ -7,6 +7,8 @@ Method names, argument meaning and error behaviour follow the reference:
 * ``GpuParser.build_tree`` / ``build_tree_reusing`` / ``download_links`` / ``GpuTree``
                                                         tree.rs:34-67, 278-290
 * ``GpuParser.search_document`` / ``search_raw`` / ``SearchResult``  search.rs:12-140
+* ``GpuParser.query_document`` / ``query_subtree`` / ``query_raw`` / ``query`` / ``QueryResult``
+                                                        document.rs:94-127, tree.rs:292-313, query.rs:10-19, 228-329
 * ``GpuParser.compile_patterns`` / ``search_many`` / ``GpuPatternSet`` / ``ManyResult``
                                                         many.rs:14-18, 76-94, 139-176, 391-399
 * limits ``MAX_PATTERN_LEN``, ``MAX_TREE_DEPTH``, ``MAX_GPU_INPUT_LEN``  lib.rs:66, tree.rs:12, util.rs:8
@@ -156,6 +158,15 @@ class GpuTree:
             self.free()
         except Exception:
             pass
+
+
+@dataclass
+class QueryResult:
+    """Result of a node query (query.rs:10-19): the number of matching lines and
+    the first ``max_matches`` of them in ascending order."""
+
+    total_matches: int
+    indices: np.ndarray
 
 
 @dataclass
@@ -389,6 +400,49 @@ class GpuParser:
                                         ctypes.byref(total), out.ctypes.data), self._ctx)
         k = min(total.value, max_matches)
         return SearchResult(total.value, out[:k].copy())
+
+    @staticmethod
+    def _filter(kind, depth) -> tuple[int, int]:
+        # query.rs:138-139: None -> 0 (any kind), None -> 0xFFFFFFFF (any depth)
+        k = 0 if kind is None else int(kind)
+        d = 0xFFFFFFFF if depth is None else int(depth)
+        return k, d
+
+    def _query_out(self, fn, *args, max_matches: int) -> QueryResult:
+        if not 0 <= max_matches <= 0xFFFFFFFF:
+            raise OnelineError(1, f"max_matches {max_matches} does not fit in u32")
+        out = np.zeros(max(max_matches, 1), np.uint32)
+        total = ctypes.c_uint32()
+        check(fn(self._ctx, *args, max_matches, ctypes.byref(total), out.ctypes.data), self._ctx)
+        return QueryResult(total.value, out[: min(total.value, max_matches)].copy())
+
+    def query_document(self, doc: GpuDocument, kind=None, depth=None, max_matches: int = 1 << 20) -> QueryResult:
+        """Lines of a resident document with the given kind and depth (document.rs:94-102)."""
+        k, d = self._filter(kind, depth)
+        return self._query_out(_lib.load().ol_query_document, doc.handle, k, d, max_matches=max_matches)
+
+    def query_subtree(self, doc: GpuDocument, tree: GpuTree, root: int, kind=None, depth=None,
+                      max_matches: int = 1 << 20) -> QueryResult:
+        """The same over the subtree of `root`, lines [root, subtree_end[root]) (tree.rs:292-313)."""
+        k, d = self._filter(kind, depth)
+        return self._query_out(_lib.load().ol_query_subtree, doc.handle, tree.handle, int(root), k, d,
+                               max_matches=max_matches)
+
+    def query_raw(self, text, kind=None, depth=None, max_matches: int = 1 << 20) -> np.ndarray:
+        """One-shot query on raw text (query.rs:230-242): the matching line indices."""
+        p, n, keep, src = _as_bytes_view(text)
+        _check_len(n)
+        k, d = self._filter(kind, depth)
+        return self._query_out(_lib.load().ol_query_raw, p, n, k, d, max_matches=max_matches).indices
+
+    def query(self, text, line_offsets, kind=None, depth=None, max_matches: int = 1 << 20) -> np.ndarray:
+        """One-shot query with line offsets computed elsewhere (query.rs:287-312)."""
+        p, n, keep, src = _as_bytes_view(text)
+        _check_len(n)
+        offs = np.ascontiguousarray(line_offsets, dtype=np.uint32)
+        k, d = self._filter(kind, depth)
+        return self._query_out(_lib.load().ol_query, p, n, offs.ctypes.data, offs.size, k, d,
+                               max_matches=max_matches).indices
 
     def compile_patterns(self, doc: GpuDocument | None, patterns, *,
                          max_patterns: int | None = MAX_PATTERNS) -> GpuPatternSet:
