@@ -82,6 +82,9 @@ ol_status ol_ctx_device_name(ol_ctx *ctx, char *buf, size_t cap);
 ol_status ol_ctx_sync(ol_ctx *ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order work. */
 void *ol_ctx_stream(ol_ctx *ctx);
+/* Kernels this library has launched in this process, over all contexts (every
+ * launch counts itself). For benchmarks; no reference counterpart. */
+uint64_t ol_launch_count(void);
 
 /* ---- resident documents: GpuParser::upload, GpuDocument::{line_count,text_len}
  *      (crates/oneline-gpu/src/document.rs:16-90, 111-127) */
@@ -196,6 +199,37 @@ ol_status ol_search_many(ol_ctx *ctx, const ol_doc *doc, const ol_patset *set, u
  * keys (0: automatic). It changes the speed, never the result. */
 ol_status ol_search_many_device(ol_ctx *ctx, const ol_doc *doc, const ol_patset *set, uint64_t max_hits,
                                 uint32_t heavy_min_hits, uint32_t *counts, uint64_t *total_hits, ol_hit *d_hits);
+
+/* ---- batches of documents. No counterpart in the reference, which handles
+ *      one document per call (GpuParser::upload / build_tree / search_many,
+ *      parser.rs:424-445, tree.rs:34-67, many.rs:391-399); per document the
+ *      results equal those calls'. The n documents are bytes
+ *      [doc_offsets[i], doc_offsets[i+1]) of data; they are laid end to end in
+ *      one resident text (a '\n' follows every non-empty document that lacks
+ *      one), parsed in one pass, linked in one pass, and searched in one pass.
+ *      Tree builds accept any depth. */
+typedef struct ol_batch ol_batch;
+ol_status ol_batch_upload(ol_ctx *ctx, const uint8_t *data, const uint64_t *doc_offsets, uint32_t n, ol_batch **out);
+void ol_batch_free(ol_batch *batch);
+uint32_t ol_batch_docs(const ol_batch *batch);
+/* Bytes of the batch text (documents and separators). */
+uint64_t ol_batch_text_len(const ol_batch *batch);
+/* Where document i lies: its bytes in the batch text and its lines. */
+ol_status ol_batch_doc_info(const ol_batch *batch, uint32_t i, uint64_t *text_start, uint64_t *text_len,
+                            uint64_t *first_line, uint64_t *line_count);
+/* parent / subtree_end / first_child / next_sibling of every document. */
+ol_status ol_batch_build_trees(ol_ctx *ctx, ol_batch *batch);
+/* Document i's offsets (from its own first byte), kinds and links (line
+ * indices within the document). Any output may be NULL. */
+ol_status ol_batch_read_doc(ol_ctx *ctx, const ol_batch *batch, uint32_t i, uint32_t *offsets, uint8_t *kinds,
+                            uint32_t *parent, uint32_t *subtree_end, uint32_t *first_child, uint32_t *next_sibling,
+                            uint64_t cap);
+/* Dictionary search of every document: hits {pattern, offset in the batch
+ * text} in (pattern, offset) order, i.e. (pattern, document, offset); no hit
+ * crosses a document. counts and *total_hits on the host, d_hits on the device
+ * (room for max_hits). */
+ol_status ol_batch_search_many(ol_ctx *ctx, const ol_batch *batch, const ol_patset *set, uint64_t max_hits,
+                               uint32_t heavy_min_hits, uint32_t *counts, uint64_t *total_hits, ol_hit *d_hits);
 
 /* ---- substring search that allocates nothing. No counterpart in the
  *      reference: an addition for callers that cannot call cudaMalloc, such as a

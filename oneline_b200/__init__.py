@@ -15,6 +15,7 @@ from .gpu import (  # noqa: F401
     MAX_PATTERNS,
     MAX_SET_PATTERN_LEN,
     MIN_SET_PATTERN_LEN,
+    GpuBatch,
     GpuDocument,
     GpuParser,
     GpuPatternSet,

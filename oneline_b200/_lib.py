@@ -35,6 +35,7 @@ SIGNATURES: dict[str, tuple] = {
     "ol_ctx_device_name": (_S, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     "ol_ctx_sync": (_S, [_P]),
     "ol_ctx_stream": (_P, [_P]),
+    "ol_launch_count": (_U64, []),
     "ol_doc_upload": (_S, [_P, _U8P, _U64, _PP]),
     "ol_doc_upload_device": (_S, [_P, _U8P, _U64, _PP]),
     "ol_doc_free": (None, [_P]),
@@ -70,6 +71,14 @@ SIGNATURES: dict[str, tuple] = {
     "ol_patset_unique": (_U32, [_P]),
     "ol_search_many": (_S, [_P, _P, _P, _U64, _P, _U64P, _P]),
     "ol_search_many_device": (_S, [_P, _P, _P, _U64, _U32, _P, _U64P, _P]),
+    "ol_batch_upload": (_S, [_P, _U8P, _P, _U32, _PP]),
+    "ol_batch_free": (None, [_P]),
+    "ol_batch_docs": (_U32, [_P]),
+    "ol_batch_text_len": (_U64, [_P]),
+    "ol_batch_doc_info": (_S, [_P, _U32, _U64P, _U64P, _U64P, _U64P]),
+    "ol_batch_build_trees": (_S, [_P, _P]),
+    "ol_batch_read_doc": (_S, [_P, _P, _U32, _P, _P, _P, _P, _P, _P, _U64]),
+    "ol_batch_search_many": (_S, [_P, _P, _P, _U64, _U32, _P, _U64P, _P]),
     "ol_search_noalloc": (_S, [_U8P, _U64, _U64, _U8P, _U32, _U32, _P, _P, _P, ctypes.c_char_p, _U32]),
 }
 

@@ -1,0 +1,99 @@
+// Batches of documents: many documents parsed, linked and searched as one
+// resident text. Documents are laid end to end, with a '\n' appended to every
+// non-empty document that does not end in one, so every document starts on a
+// line of its own and keeps exactly its own lines, kinds and depths. These
+// kernels keep the tree links and the search hits from crossing a document
+// boundary. The reference has no batch form: it parses one document per call
+// (crates/oneline-gpu/src/parser.rs:424-445); the per-document semantics are
+// those of core links.rs:52-82 and simd search.rs:259-282.
+#include <cuda_runtime.h>
+
+#include "ol_common.cuh"
+#include "ol_kernels.h"
+
+namespace ol {
+
+// line_start[i] = the first line at or after document i's first byte (its
+// first line when it has any); line_start[n] = L.
+__global__ void batch_line_starts_kernel(const uint32_t *__restrict__ offsets, uint32_t L,
+                                         const unsigned long long *__restrict__ seg_start, uint32_t n,
+                                         uint32_t *__restrict__ line_start) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    if (i == n) {
+        line_start[n] = L;
+        return;
+    }
+    const unsigned long long s = seg_start[i];
+    uint32_t lo = 0, hi = L;  // first line with offset >= s
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((unsigned long long)__ldg(offsets + mid) < s)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    line_start[i] = lo;
+}
+
+// The document of line j: the last i with line_start[i] <= j among documents
+// that have lines (empty documents share their successor's start).
+__device__ __forceinline__ uint32_t doc_of_line(const uint32_t *line_start, uint32_t n, uint32_t j) {
+    uint32_t lo = 0, hi = n;  // last i in [0, n) with line_start[i] <= j
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(line_start + mid) <= j)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Tree links of the whole text restricted to each line's document: a parent
+// before the document becomes NONE, a subtree end past it becomes the
+// document's end, a first child past it NONE, and next_sibling is recomputed
+// from the restricted links (parents equal after restriction).
+//
+// It may run in place (outputs = inputs): a thread reads another line's parent
+// only inside its own document, where the raw and the restricted parent
+// restrict to the same value.
+__global__ void batch_tree_fixup_kernel(const uint32_t *__restrict__ line_start, uint32_t n, uint32_t L,
+                                        const uint8_t *__restrict__ kinds, const uint32_t *parent_in,
+                                        const uint32_t *end_in, const uint32_t *fc_in, uint32_t *parent,
+                                        uint32_t *subtree_end, uint32_t *first_child, uint32_t *next_sibling) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= L) return;
+    const uint32_t d = doc_of_line(line_start, n, j);
+    const uint32_t ls = __ldg(line_start + d), le = __ldg(line_start + d + 1);  // d is the last start <= j
+    auto clamp_parent = [&](uint32_t p) { return (p != NONE && p >= ls) ? p : NONE; };
+    const uint32_t p = clamp_parent(parent_in[j]);
+    const uint32_t e = min(end_in[j], le);
+    const uint32_t f = fc_in[j];
+    uint32_t ns = NONE;
+    // blank lines have no siblings; otherwise the end is a sibling when it lies
+    // in the document and the restricted parents agree
+    if (__ldg(kinds + j) != KIND_BLANK && e < le && clamp_parent(parent_in[e]) == p) ns = e;
+    parent[j] = p;
+    subtree_end[j] = e;
+    first_child[j] = (f != NONE && f < le) ? f : NONE;
+    next_sibling[j] = ns;
+}
+
+cudaError_t launch_batch_line_starts(const uint32_t *offsets, uint32_t L, const unsigned long long *seg_start, uint32_t n,
+                                     uint32_t *line_start, cudaStream_t st) {
+    batch_line_starts_kernel<<<(n + 1 + 255) / 256, 256, 0, st>>>(offsets, L, seg_start, n, line_start); OL_LAUNCHED();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_tree_fixup(const uint32_t *line_start, uint32_t n, uint32_t L, const uint8_t *kinds,
+                                    const uint32_t *parent_in,
+                                    const uint32_t *end_in, const uint32_t *fc_in, uint32_t *parent, uint32_t *subtree_end,
+                                    uint32_t *first_child, uint32_t *next_sibling, cudaStream_t st) {
+    if (L == 0 || n == 0) return cudaSuccess;
+    batch_tree_fixup_kernel<<<(L + 255) / 256, 256, 0, st>>>(line_start, n, L, kinds, parent_in, end_in, fc_in, parent,
+                                                             subtree_end, first_child, next_sibling); OL_LAUNCHED();
+    return cudaGetLastError();
+}
+
+}  // namespace ol

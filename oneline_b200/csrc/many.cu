@@ -35,19 +35,21 @@ namespace ol {
 
 constexpr uint32_t DM_THREADS = 256;
 constexpr uint32_t DM_WARPS = DM_THREADS / 32;
-constexpr uint32_t DM_POS_PER_WARP = kDictTile / DM_WARPS;  // 2048
-constexpr uint32_t DM_STEPS = DM_POS_PER_WARP / 32;          // 64
-constexpr uint32_t DM_FLUSH = 8;                              // bitmap words staged per heavy pattern
+constexpr uint32_t DM_SLICE = 512;                        // text positions per warp work item
+constexpr uint32_t DM_SLICE_WORDS = DM_SLICE / 32;        // bitmap words per slice
+constexpr uint32_t DM_SLICES_PER_TILE = kDictTile / DM_SLICE;
+constexpr uint32_t DM_TEXT_BYTES = DM_SLICE + kDictHalo;  // staged per slice
+constexpr uint32_t DM_QCAP = 64;                          // per-warp candidate queue
 constexpr uint32_t DM_FILTER_WORDS = 1u << (kDictFilterBits - 5);
-constexpr uint32_t DM_TEXT_BYTES = kDictTile + kDictHalo;
 constexpr uint32_t kMbarSpins = 1u << 24;
-static_assert(DM_STEPS % DM_FLUSH == 0, "flush windows");
 static_assert(DM_TEXT_BYTES % 16 == 0, "16-byte staging");
+static_assert(kDictWordsPerTile % DM_SLICE_WORDS == 0, "slices tile the bitmap");
 
 struct DictSmem {
     uint32_t filter[DM_FILTER_WORDS];
-    alignas(16) uint8_t text[DM_TEXT_BYTES];
-    uint32_t stage[DM_WARPS][kDictMaxHeavy * DM_FLUSH];
+    alignas(16) uint8_t text[DM_WARPS][DM_TEXT_BYTES];
+    uint32_t stage[DM_WARPS][kDictMaxHeavy * DM_SLICE_WORDS];  // heavy bitmap words of the warp's slice
+    uint16_t queue[DM_WARPS][DM_QCAP];
     alignas(8) unsigned long long bar;
 };
 
@@ -117,6 +119,57 @@ __device__ __forceinline__ uint32_t dict_probe(const DictSet &s, uint32_t key) {
 
 // ------------------------------------------------------------- matching ----
 
+// Emits unique pattern u at absolute offset pos (slice-local position p).
+__device__ __forceinline__ void dict_emit(const DictMatchArgs &a, uint32_t *stage, uint32_t u, uint64_t pos, uint32_t p) {
+    if (a.count_only) {
+        const uint32_t peers = __match_any_sync(__activemask(), u);
+        if ((peers & ((1u << (threadIdx.x & 31)) - 1u)) == 0) atomicAdd(a.counts + u, (uint32_t)__popc(peers));
+        return;
+    }
+    const uint32_t hv = __ldg(a.heavy_of_u + u);
+    if (hv != 0xFFu) {
+        atomicOr(stage + hv * DM_SLICE_WORDS + (p >> 5), 1u << (p & 31));
+    } else {
+        atomicAdd(a.counts + u, 1u);
+        const uint32_t slot = atomicAdd(a.light_n, 1u);
+        if (slot < a.light_cap) a.light_keys[slot] = ((unsigned long long)u << 32) | (uint32_t)pos;
+    }
+}
+
+// Every unique pattern starting at slice position p: probe the table with the
+// position's first four bytes, then walk the trie byte by byte. Hits must end
+// by `lim` (the end of the text, or of the position's document in a batch).
+__device__ __forceinline__ void dict_walk(const DictMatchArgs &a, const uint8_t *text, uint32_t *stage, uint32_t p,
+                                          uint64_t pos, uint64_t lim) {
+    const uint32_t key = (uint32_t)text[p] | ((uint32_t)text[p + 1] << 8) | ((uint32_t)text[p + 2] << 16) |
+                         ((uint32_t)text[p + 3] << 24);
+    uint32_t v = pos + kDictMinLen <= lim ? dict_probe(a.set, key) : NONE;
+    uint32_t d = kDictMinLen;
+    while (v != NONE) {
+        const uint4 nd = __ldg(a.set.nodes + v);
+        if (nd.x != NONE) dict_emit(a, stage, nd.x, pos, p);
+        if (d >= kDictMaxLen || pos + d >= lim) break;
+        v = dict_child(a.set, nd, text[p + d]);
+        d++;
+    }
+}
+
+// End of the document holding pos (pos itself when pos lies between
+// documents), searching forward from hint, the first document ending after the
+// slice start.
+__device__ __forceinline__ uint64_t dict_limit(const DictMatchArgs &a, uint64_t pos, uint32_t hint) {
+    if (!a.seg_end) return a.text_len;
+    uint32_t i = hint;
+    while (i < a.n_seg && a.seg_end[i] <= pos) i++;
+    if (i == a.n_seg || a.seg_start[i] > pos) return pos;
+    return a.seg_end[i];
+}
+
+// Each warp takes slices of 512 positions in turn: it stages the slice (plus
+// the longest pattern) in its own shared memory, filters all positions 32 at a
+// time, queues the candidates and walks them 32 at a time (one per lane), so
+// walks run on full warps; heavy hits set bits in the slice's staged bitmap
+// words, written out once per slice. Warps never wait for one another.
 __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a) {
     extern __shared__ __align__(16) uint8_t dyn_smem[];
     DictSmem &sm = *reinterpret_cast<DictSmem *>(dyn_smem);
@@ -137,77 +190,66 @@ __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a)
         return;
     }
 
-    const uint32_t n_work = (a.n_tiles + a.tile_stride - 1) / a.tile_stride;
     const uint64_t N = a.text_len;
     const uint32_t n_words = a.n_tiles * kDictWordsPerTile;
+    const uint32_t n_items = ((a.n_tiles + a.tile_stride - 1) / a.tile_stride) * DM_SLICES_PER_TILE;
+    const uint32_t H = a.count_only ? 0u : a.n_heavy;
+    uint8_t *text = sm.text[warp];
     uint32_t *stage = sm.stage[warp];
-    const uint32_t H = a.n_heavy;
+    uint16_t *queue = sm.queue[warp];
 
-    for (uint32_t k = blockIdx.x; k < n_work; k += gridDim.x) {
-        const uint32_t tile = k * a.tile_stride;
-        const uint64_t t0 = (uint64_t)tile * kDictTile;
-        __syncthreads();  // the previous tile's text is no longer read
-        for (uint32_t o = tid * 16; o < DM_TEXT_BYTES; o += DM_THREADS * 16)
-            *reinterpret_cast<uint4 *>(&sm.text[o]) = ld_stream16(a.text + t0 + o);
-        __syncthreads();
-        const uint32_t *tw = reinterpret_cast<const uint32_t *>(sm.text);
-
-        for (uint32_t s = 0; s < DM_STEPS; s++) {
-            if (!a.count_only && (s % DM_FLUSH) == 0) {
-                for (uint32_t f = lane; f < H * DM_FLUSH; f += 32) stage[f] = 0;
-                __syncwarp();
+    for (uint32_t item = blockIdx.x * DM_WARPS + warp; item < n_items; item += gridDim.x * DM_WARPS) {
+        const uint32_t slice = (item / DM_SLICES_PER_TILE) * a.tile_stride * DM_SLICES_PER_TILE + item % DM_SLICES_PER_TILE;
+        const uint64_t s0 = (uint64_t)slice * DM_SLICE;  // slices past the text only write zero words
+        __syncwarp();
+        for (uint32_t o = lane * 16; o < DM_TEXT_BYTES; o += 32 * 16)
+            *reinterpret_cast<uint4 *>(&text[o]) = ld_stream16(a.text + s0 + o);
+        for (uint32_t f = lane; f < H * DM_SLICE_WORDS; f += 32) stage[f] = 0;
+        __syncwarp();
+        const uint32_t *tw = reinterpret_cast<const uint32_t *>(text);
+        uint32_t hint = 0;
+        if (a.seg_end) {  // first document ending after the slice start
+            uint32_t lo = 0, hi = a.n_seg;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (a.seg_end[mid] <= s0)
+                    lo = mid + 1;
+                else
+                    hi = mid;
             }
-            const uint32_t p = warp * DM_POS_PER_WARP + s * 32 + lane;  // tile-local position
-            const uint64_t pos = t0 + p;
-            uint32_t v = NONE;
+            hint = lo;
+        }
+        uint32_t qn = 0;
+        for (uint32_t step = 0; step < DM_SLICE / 32; step++) {
+            const uint32_t p = step * 32 + lane;
+            const uint64_t pos = s0 + p;
+            bool cand = false;
             if (pos + kDictMinLen <= N) {
                 const uint32_t key = __funnelshift_r(tw[p >> 2], tw[(p >> 2) + 1], (p & 3) * 8);
                 const uint32_t h1 = dict_filter_h1(key), h2 = dict_filter_h2(key);
-                if (((sm.filter[h1 >> 5] >> (h1 & 31)) & (sm.filter[h2 >> 5] >> (h2 & 31)) & 1u) != 0)
-                    v = dict_probe(a.set, key);
+                cand = ((sm.filter[h1 >> 5] >> (h1 & 31)) & (sm.filter[h2 >> 5] >> (h2 & 31)) & 1u) != 0;
             }
-            uint32_t d = kDictMinLen;
-            while (__any_sync(0xFFFFFFFFu, v != NONE)) {
-                uint4 nd = make_uint4(NONE, 0, 0, 0);
-                if (v != NONE) nd = __ldg(a.set.nodes + v);
-                const uint32_t u = nd.x;
-                const bool emit = u != NONE && pos + d <= N;
-                const uint32_t em = __ballot_sync(0xFFFFFFFFu, emit);
-                if (emit) {
-                    const uint32_t peers = __match_any_sync(em, u);
-                    const bool leader = (peers & lt) == 0;
-                    if (a.count_only) {
-                        if (leader) atomicAdd(a.counts + u, (uint32_t)__popc(peers));
-                    } else {
-                        const uint32_t hv = __ldg(a.heavy_of_u + u);
-                        const bool light = hv == 0xFFu;
-                        if (!light && leader) stage[hv * DM_FLUSH + (s % DM_FLUSH)] = peers;
-                        const uint32_t lm = __ballot_sync(em, light);
-                        if (light) {
-                            if (leader) atomicAdd(a.counts + u, (uint32_t)__popc(peers));
-                            const uint32_t first = __ffs(lm) - 1;
-                            uint32_t base = 0;
-                            if (lane == first) base = atomicAdd(a.light_n, (uint32_t)__popc(lm));
-                            base = __shfl_sync(lm, base, first);
-                            const uint32_t slot = base + __popc(lm & lt);
-                            if (slot < a.light_cap) a.light_keys[slot] = ((unsigned long long)u << 32) | (uint32_t)pos;
-                        }
-                    }
-                }
-                uint32_t nv = NONE;
-                if (v != NONE && d < kDictMaxLen && pos + d < N) nv = dict_child(a.set, nd, sm.text[p + d]);
-                v = nv;
-                d++;
-            }
-            if (!a.count_only && (s % DM_FLUSH) == DM_FLUSH - 1) {
+            const uint32_t cm = __ballot_sync(0xFFFFFFFFu, cand);
+            if (cand) queue[qn + __popc(cm & lt)] = (uint16_t)p;
+            qn += __popc(cm);
+            __syncwarp();
+            if (qn >= 32) {  // walk 32 candidates, one per lane
+                const uint32_t q = queue[lane];
+                dict_walk(a, text, stage, q, s0 + q, dict_limit(a, s0 + q, hint));
                 __syncwarp();
-                // words [wbase, wbase + 8) of every heavy bitmap: 32-byte sectors
-                const uint32_t wbase = tile * kDictWordsPerTile + warp * (DM_POS_PER_WARP / 32) + (s - (DM_FLUSH - 1));
-                for (uint32_t f = lane; f < H * DM_FLUSH; f += 32)
-                    a.bitmap[(size_t)(f / DM_FLUSH) * n_words + wbase + (f % DM_FLUSH)] = stage[f];
+                const uint16_t keep = lane + 32 < qn ? queue[lane + 32] : (uint16_t)0;
+                __syncwarp();
+                if (lane + 32 < qn) queue[lane] = keep;
+                qn -= 32;
                 __syncwarp();
             }
         }
+        if (lane < qn) dict_walk(a, text, stage, queue[lane], s0 + queue[lane], dict_limit(a, s0 + queue[lane], hint));
+        __syncwarp();
+        // the slice's heavy bitmap words: 64 contiguous bytes per pattern
+        const uint32_t w0 = slice * DM_SLICE_WORDS;
+        for (uint32_t f = lane; f < H * DM_SLICE_WORDS; f += 32)
+            a.bitmap[(size_t)(f / DM_SLICE_WORDS) * n_words + w0 + (f % DM_SLICE_WORDS)] = stage[f];
     }
 }
 
@@ -219,9 +261,10 @@ cudaError_t launch_dict_match(const DictMatchArgs &a, int sm_count, cudaStream_t
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dict_match_kernel, DM_THREADS, smem);
     if (e != cudaSuccess) return e;
-    const uint32_t n_work = (a.n_tiles + a.tile_stride - 1) / a.tile_stride;
-    const uint32_t grid = (uint32_t)std::min<uint64_t>(n_work, (uint64_t)std::max(per_sm, 1) * sm_count);
-    dict_match_kernel<<<grid, DM_THREADS, smem, st>>>(a);
+    const uint64_t n_items = (uint64_t)((a.n_tiles + a.tile_stride - 1) / a.tile_stride) * DM_SLICES_PER_TILE;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((n_items + DM_WARPS - 1) / DM_WARPS,
+                                                       (uint64_t)std::max(per_sm, 1) * sm_count);
+    dict_match_kernel<<<grid, DM_THREADS, smem, st>>>(a); OL_LAUNCHED();
     return cudaGetLastError();
 }
 
@@ -280,7 +323,7 @@ cudaError_t launch_dict_heavy_count(const uint32_t *bitmap, uint32_t n_words, ui
                                     uint32_t ld, cudaStream_t st) {
     if (n_heavy == 0 || n_words == 0) return cudaSuccess;
     dim3 grid(dict_heavy_blocks(n_words), n_heavy);
-    dict_heavy_count_kernel<<<grid, DH_THREADS, 0, st>>>(bitmap, n_words, counts, ld);
+    dict_heavy_count_kernel<<<grid, DH_THREADS, 0, st>>>(bitmap, n_words, counts, ld); OL_LAUNCHED();
     return cudaGetLastError();
 }
 
@@ -363,10 +406,10 @@ cudaError_t launch_dict_sort(unsigned long long *keys, unsigned long long *tmp, 
     passes += passes & 1;  // an even number of passes leaves the result in keys
     for (uint32_t p = 0; p < passes; p++) {
         const uint32_t shift = 8 * p;
-        dict_sort_hist_kernel<<<blocks, DS_THREADS, 0, st>>>(src, n, shift, counts, ld, chunks);
+        dict_sort_hist_kernel<<<blocks, DS_THREADS, 0, st>>>(src, n, shift, counts, ld, chunks); OL_LAUNCHED();
         cudaError_t e = launch_scan_columns(counts, bases, totals, chunks, 256, ld, st);
         if (e != cudaSuccess) return e;
-        dict_sort_scatter_kernel<<<blocks, DS_THREADS, 0, st>>>(src, dst, n, shift, bases, totals, ld, chunks);
+        dict_sort_scatter_kernel<<<blocks, DS_THREADS, 0, st>>>(src, dst, n, shift, bases, totals, ld, chunks); OL_LAUNCHED();
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         unsigned long long *t = src;
         src = dst;
@@ -443,44 +486,89 @@ __global__ void __launch_bounds__(DI_THREADS) dict_ids_kernel(DictEmitArgs a) {
 }
 
 cudaError_t launch_dict_ids(const DictEmitArgs &a, cudaStream_t st) {
-    dict_ids_kernel<<<1, DI_THREADS, 0, st>>>(a);
+    dict_ids_kernel<<<1, DI_THREADS, 0, st>>>(a); OL_LAUNCHED();
     return cudaGetLastError();
 }
 
 // ----------------------------------------------------------------- emit ----
 
-// Heavy hits: block (b, h) expands words [4096b, 4096b + 4096) of bitmap h;
-// thread t owns 16 consecutive words, its first rank from a block scan.
+// Position of the k-th (0-based) set bit of w; w has more than k set bits.
+__device__ __forceinline__ uint32_t select_bit(uint32_t w, uint32_t k) {
+    uint32_t r = 0, c;
+    c = __popc(w & 0xFFFFu);
+    if (k >= c) { k -= c; w >>= 16; r += 16; }
+    c = __popc(w & 0xFFu);
+    if (k >= c) { k -= c; w >>= 8; r += 8; }
+    c = __popc(w & 0xFu);
+    if (k >= c) { k -= c; w >>= 4; r += 4; }
+    c = __popc(w & 0x3u);
+    if (k >= c) { k -= c; w >>= 2; r += 2; }
+    c = w & 1u;
+    if (k >= c) r += 1;
+    return r;
+}
+
+// Heavy hits: block (b, h) expands words [4096b, 4096b + 4096) of bitmap h,
+// warp w the 512 words [4096b + 512w, ...), 32 words per round. A round's hits
+// are written by the whole warp to consecutive slots: lane j of each 32 finds
+// its word by a binary search over the round's word prefix sums and its bit by
+// select, so every store instruction covers 32 consecutive hits.
 __global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArgs a) {
-    __shared__ uint32_t warp_sum[DH_THREADS / 32];
+    __shared__ uint32_t warp_tot[DH_THREADS / 32];
     const uint32_t h = blockIdx.y, b = blockIdx.x;
-    const uint32_t w0 = b * DH_WORDS + threadIdx.x * DH_WORDS_PER_THREAD;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t *col = a.bitmap + (size_t)h * a.n_words;
+    const uint32_t w0 = b * DH_WORDS + warp * (DH_WORDS / (DH_THREADS / 32));
+    constexpr uint32_t kRounds = DH_WORDS / (DH_THREADS / 32) / 32;  // 16
     uint32_t c = 0;
-    if (w0 < a.n_words) {
-#pragma unroll
-        for (uint32_t i = 0; i < DH_WORDS_PER_THREAD; i += 4) {
-            uint4 q = __ldg(reinterpret_cast<const uint4 *>(col + w0 + i));
-            c += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
-        }
+    for (uint32_t r = 0; r < kRounds; r++) {
+        const uint32_t idx = w0 + r * 32 + lane;
+        c += idx < a.n_words ? __popc(__ldg(col + idx)) : 0u;
     }
-    uint32_t rank = a.heavy_bases[(size_t)h * a.ld + b] + block_exclusive_256(c, warp_sum, nullptr);
-    if (c == 0) return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    if (lane == 0) warp_tot[warp] = c;
+    __syncthreads();
+    uint32_t rank = a.heavy_bases[(size_t)h * a.ld + b];
+    for (uint32_t w = 0; w < warp; w++) rank += warp_tot[w];
+    if (c == 0) return;  // uniform over the warp
     const uint32_t u = a.heavy_u[h];
     const uint32_t d0 = a.dup_start[u], d1 = a.dup_start[u + 1];
-    for (uint32_t i = 0; i < DH_WORDS_PER_THREAD; i++) {
-        uint32_t bits = __ldg(col + w0 + i);  // again: the words were just read
-        while (bits) {
-            const uint32_t bit = __ffs(bits) - 1;
-            bits &= bits - 1;
-            const uint32_t off = (w0 + i) * 32 + bit;
-            for (uint32_t d = d0; d < d1; d++) {
-                const uint32_t id = a.dup_ids[d];
-                const unsigned long long slot = a.id_base[id] + rank;
-                if (slot < a.max_hits) a.hits[slot] = make_uint2(id, off);
-            }
-            rank++;
+    const uint32_t lt = (1u << lane) - 1u;
+    (void)lt;
+    for (uint32_t r = 0; r < kRounds; r++) {
+        const uint32_t idx = w0 + r * 32 + lane;
+        const uint32_t word = idx < a.n_words ? __ldg(col + idx) : 0u;
+        const uint32_t cnt = __popc(word);
+        uint32_t inc = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if ((int)lane >= o) inc += t;
         }
+        const uint32_t excl = inc - cnt;
+        const uint32_t T = __shfl_sync(0xFFFFFFFFu, inc, 31);
+        for (uint32_t base = 0; base < T; base += 32) {
+            const uint32_t j = base + lane;
+            // largest word i of the round with excl[i] <= j: it holds hit j
+            uint32_t i = 0;
+#pragma unroll
+            for (uint32_t step = 16; step > 0; step >>= 1) {
+                const uint32_t e = __shfl_sync(0xFFFFFFFFu, excl, i + step);
+                if (e <= j) i += step;
+            }
+            const uint32_t wi = __shfl_sync(0xFFFFFFFFu, word, i);
+            const uint32_t ei = __shfl_sync(0xFFFFFFFFu, excl, i);
+            if (j < T) {
+                const uint32_t off = (w0 + r * 32 + i) * 32 + select_bit(wi, j - ei);
+                for (uint32_t d = d0; d < d1; d++) {
+                    const uint32_t id = __ldg(a.dup_ids + d);
+                    const unsigned long long slot = a.id_base[id] + rank + j;
+                    if (slot < a.max_hits) a.hits[slot] = make_uint2(id, off);
+                }
+            }
+        }
+        rank += T;
     }
 }
 
@@ -502,12 +590,12 @@ cudaError_t launch_dict_emit(const DictEmitArgs &a, cudaStream_t st) {
     if (a.max_hits == 0) return cudaSuccess;
     if (a.n_heavy && a.n_words) {
         dim3 grid(dict_heavy_blocks(a.n_words), a.n_heavy);
-        dict_emit_heavy_kernel<<<grid, DH_THREADS, 0, st>>>(a);
+        dict_emit_heavy_kernel<<<grid, DH_THREADS, 0, st>>>(a); OL_LAUNCHED();
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     if (a.light_n) {
-        dict_emit_light_kernel<<<(a.light_n + 255) / 256, 256, 0, st>>>(a);
+        dict_emit_light_kernel<<<(a.light_n + 255) / 256, 256, 0, st>>>(a); OL_LAUNCHED();
         return cudaGetLastError();
     }
     return cudaSuccess;

@@ -7,6 +7,11 @@
 
 namespace ol {
 
+// Kernels launched by this library in this process (every launch site counts
+// itself), read through ol_launch_count().
+void count_launch();
+#define OL_LAUNCHED() ::ol::count_launch()
+
 struct FlatNode;
 struct DocStats;
 
@@ -166,6 +171,11 @@ struct DictMatchArgs {
     uint32_t light_cap;
     uint32_t *light_n;
     uint32_t *error;
+    // Batches: hits must lie inside one document, [seg_start[i], seg_end[i])
+    // (sorted, disjoint); nullptr: the whole text is one document.
+    const unsigned long long *seg_start;
+    const unsigned long long *seg_end;
+    uint32_t n_seg;
 };
 
 cudaError_t launch_dict_match(const DictMatchArgs &a, int sm_count, cudaStream_t st);
@@ -202,6 +212,14 @@ struct DictEmitArgs {
     unsigned long long max_hits;
 };
 cudaError_t launch_dict_ids(const DictEmitArgs &a, cudaStream_t st);
+
+// Batches (batch.cu).
+cudaError_t launch_batch_line_starts(const uint32_t *offsets, uint32_t L, const unsigned long long *seg_start, uint32_t n,
+                                     uint32_t *line_start, cudaStream_t st);
+cudaError_t launch_batch_tree_fixup(const uint32_t *line_start, uint32_t n, uint32_t L, const uint8_t *kinds,
+                                    const uint32_t *parent_in, const uint32_t *end_in, const uint32_t *fc_in,
+                                    uint32_t *parent, uint32_t *subtree_end, uint32_t *first_child,
+                                    uint32_t *next_sibling, cudaStream_t st);
 cudaError_t launch_dict_emit(const DictEmitArgs &a, cudaStream_t st);
 
 }  // namespace ol

@@ -328,21 +328,21 @@ __global__ void classify_lines_kernel(const uint8_t *__restrict__ text, uint64_t
 
 cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st) {
     if (a.n_tiles == 0) return cudaSuccess;
-    newline_count_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a.text, a.text_len, a.tile_count);
+    newline_count_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a.text, a.text_len, a.tile_count); OL_LAUNCHED();
     cudaError_t e = launch_scan_columns(a.tile_count, a.tile_base, nullptr, a.n_tiles, 1, scan_ld(a.n_tiles), st);
     if (e != cudaSuccess) return e;
-    parse_tiles_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a);
+    parse_tiles_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a); OL_LAUNCHED();
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     uint32_t blocks = a.fixup_cap < 64 ? 8 : 64;
-    parse_fixup_kernel<<<blocks, 256, 0, st>>>(a);
+    parse_fixup_kernel<<<blocks, 256, 0, st>>>(a); OL_LAUNCHED();
     return cudaGetLastError();
 }
 
 cudaError_t launch_classify_lines(const uint8_t *text, uint64_t N, const uint32_t *offsets, uint32_t L, FlatNode *nodes,
                                   uint32_t *depth32, cudaStream_t st) {
     if (L == 0) return cudaSuccess;
-    classify_lines_kernel<<<(L + 255) / 256, 256, 0, st>>>(text, N, offsets, L, nodes, depth32);
+    classify_lines_kernel<<<(L + 255) / 256, 256, 0, st>>>(text, N, offsets, L, nodes, depth32); OL_LAUNCHED();
     return cudaGetLastError();
 }
 

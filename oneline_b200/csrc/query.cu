@@ -96,10 +96,10 @@ __global__ void __launch_bounds__(QY_THREADS) query_write_kernel(QueryArgs a) {
 cudaError_t launch_query(const QueryArgs &a, cudaStream_t st) {
     if (a.hi <= a.lo) return cudaSuccess;
     const uint32_t blocks = query_blocks(a.hi - a.lo);
-    query_count_kernel<<<blocks, QY_THREADS, 0, st>>>(a);
+    query_count_kernel<<<blocks, QY_THREADS, 0, st>>>(a); OL_LAUNCHED();
     cudaError_t e = launch_scan_columns(a.counts, a.bases, a.total, blocks, 1, scan_ld(blocks), st);
     if (e != cudaSuccess) return e;
-    query_write_kernel<<<blocks, QY_THREADS, 0, st>>>(a);
+    query_write_kernel<<<blocks, QY_THREADS, 0, st>>>(a); OL_LAUNCHED();
     return cudaGetLastError();
 }
 

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -24,6 +25,9 @@ using namespace ol;
 // ------------------------------------------------------------ utilities ----
 
 namespace ol {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 ol_status ctx_fail(ol_ctx *ctx, ol_status code, const std::string &msg) {
     if (ctx) ctx->last_error = msg;
@@ -492,3 +496,5 @@ ol_status ol::new_text_doc(ol_ctx *ctx, const uint8_t *text, uint64_t len, ol_do
     *out = d;
     return OL_OK;
 }
+
+extern "C" uint64_t ol_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }

@@ -1,0 +1,237 @@
+// C ABI for batches of documents (no reference counterpart: the reference
+// parses, links and searches one document per call, parser.rs:424-445,
+// tree.rs:34-67, many.rs:391-399). A batch lays its documents end to end in
+// one resident text, with a '\n' after every non-empty document that lacks
+// one, so that every document's lines, kinds and depths are exactly its own;
+// one parse, one tree build and one dictionary pass then cover all documents,
+// and batch kernels keep tree links and hits inside their document.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "runtime.h"
+
+using namespace ol;
+
+struct ol_batch {
+    ol_ctx *ctx = nullptr;
+    ol_doc *doc = nullptr;        // the concatenated text, parsed
+    ol_tree *tree = nullptr;      // per-document links once built
+    uint32_t n = 0;
+    std::vector<uint64_t> start;  // document i: bytes [start[i], start[i] + len[i]) of the text
+    std::vector<uint64_t> len;
+    std::vector<uint32_t> line_start;  // n + 1 entries
+    DevBuf table;                 // device: seg_start[n], seg_end[n] (u64), line_start[n + 1] (u32)
+    const unsigned long long *seg_start = nullptr, *seg_end = nullptr;
+    uint32_t *d_line_start = nullptr;
+};
+
+extern "C" ol_status ol_batch_upload(ol_ctx *ctx, const uint8_t *data, const uint64_t *doc_offsets, uint32_t n,
+                                     ol_batch **out) {
+    if (!ctx || !out || !doc_offsets || n == 0) return OL_ERR_INVALID_ARG;
+    *out = nullptr;
+    for (uint32_t i = 0; i < n; i++)
+        if (doc_offsets[i + 1] < doc_offsets[i]) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "document offsets must not decrease");
+    if (doc_offsets[n] > doc_offsets[0] && !data) return OL_ERR_INVALID_ARG;
+    // Layout: document bytes, then '\n' when the document is non-empty and does
+    // not already end in one.
+    auto b = new ol_batch();
+    b->ctx = ctx;
+    b->n = n;
+    b->start.resize(n);
+    b->len.resize(n);
+    uint64_t T = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        const uint64_t l = doc_offsets[i + 1] - doc_offsets[i];
+        b->start[i] = T;
+        b->len[i] = l;
+        T += l + ((l && data[doc_offsets[i + 1] - 1] != '\n') ? 1 : 0);
+    }
+    if (T > OL_MAX_GPU_INPUT_LEN) {
+        delete b;
+        return ctx_fail(ctx, OL_ERR_INPUT_TOO_LARGE, "batch text of " + std::to_string(T) + " bytes exceeds the 32-bit limit");
+    }
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    ol_status s = new_doc(ctx, T, &b->doc);
+    cudaError_t e = cudaSuccess;
+    // Pack through the pinned ring: documents and separators, 16 MiB per copy.
+    uint64_t at = 0, ring_i = 0, fill = 0;
+    uint8_t *slot = nullptr;
+    auto flush = [&]() -> cudaError_t {
+        if (!fill) return cudaSuccess;
+        int k = (int)(ring_i % kRingSlots);
+        cudaError_t r = cudaMemcpyAsync(b->doc->text + at, slot, fill, cudaMemcpyHostToDevice, st);
+        if (r == cudaSuccess) r = cudaEventRecord(ctx->ring_done[k], st);
+        at += fill;
+        fill = 0;
+        ring_i++;
+        slot = nullptr;
+        return r;
+    };
+    auto put = [&](const uint8_t *src, uint64_t nbytes) -> cudaError_t {
+        while (nbytes) {
+            if (!slot) {
+                int k = (int)(ring_i % kRingSlots);
+                cudaError_t r = cudaEventSynchronize(ctx->ring_done[k]);
+                if (r != cudaSuccess) return r;
+                slot = ctx->ring[k];
+            }
+            const uint64_t c = std::min<uint64_t>(nbytes, kRingBytes - fill);
+            memcpy(slot + fill, src, c);
+            fill += c;
+            src += c;
+            nbytes -= c;
+            if (fill == kRingBytes) {
+                cudaError_t r = flush();
+                if (r != cudaSuccess) return r;
+            }
+        }
+        return cudaSuccess;
+    };
+    static const uint8_t nl = '\n';
+    for (uint32_t i = 0; s == OL_OK && e == cudaSuccess && i < n; i++) {
+        const uint64_t l = b->len[i];
+        if (l) e = put(data + doc_offsets[i], l);
+        if (e == cudaSuccess && l && data[doc_offsets[i + 1] - 1] != '\n') e = put(&nl, 1);
+    }
+    if (s == OL_OK && e == cudaSuccess) e = flush();
+    if (s == OL_OK && e != cudaSuccess) s = ctx_cuda(ctx, e, "batch upload");
+    if (s == OL_OK && T) s = parse_doc(ctx, b->doc, T / 24 + 4096, nullptr);
+    // Document ranges and first lines on the device.
+    const size_t tbytes = (size_t)n * 16 + (size_t)(n + 1) * 4;
+    if (s == OL_OK) {
+        std::vector<uint8_t> host(tbytes);
+        std::vector<uint64_t> ends(n);
+        for (uint32_t i = 0; i < n; i++) ends[i] = b->start[i] + b->len[i];
+        memcpy(host.data(), b->start.data(), (size_t)n * 8);
+        memcpy(host.data() + (size_t)n * 8, ends.data(), (size_t)n * 8);
+        e = b->table.reserve(tbytes, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b->table.ptr, host.data(), (size_t)n * 16, cudaMemcpyHostToDevice, st);
+        b->seg_start = (const unsigned long long *)b->table.ptr;
+        b->seg_end = b->seg_start + n;
+        b->d_line_start = (uint32_t *)((uint8_t *)b->table.ptr + (size_t)n * 16);
+        if (e == cudaSuccess)
+            e = launch_batch_line_starts(b->doc->offsets, b->doc->line_count, b->seg_start, n, b->d_line_start, st);
+        b->line_start.resize(n + 1);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->line_start.data(), b->d_line_start, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) s = ctx_cuda(ctx, e, "batch tables");
+    }
+    if (s != OL_OK) {
+        ol_batch_free(b);
+        return s;
+    }
+    *out = b;
+    return OL_OK;
+}
+
+extern "C" void ol_batch_free(ol_batch *b) {
+    if (!b) return;
+    if (b->tree) ol_tree_free(b->tree);
+    if (b->doc) ol_doc_free(b->doc);
+    if (b->ctx) {
+        std::lock_guard<std::recursive_mutex> g(b->ctx->mu);
+        cudaSetDevice(b->ctx->device);
+        b->table.release(b->ctx->stream);
+    }
+    delete b;
+}
+
+extern "C" uint32_t ol_batch_docs(const ol_batch *b) { return b ? b->n : 0; }
+
+extern "C" uint64_t ol_batch_text_len(const ol_batch *b) { return b && b->doc ? b->doc->text_len : 0; }
+
+extern "C" ol_status ol_batch_doc_info(const ol_batch *b, uint32_t i, uint64_t *text_start, uint64_t *text_len,
+                                       uint64_t *first_line, uint64_t *line_count) {
+    if (!b || i >= b->n) return OL_ERR_INVALID_ARG;
+    if (text_start) *text_start = b->start[i];
+    if (text_len) *text_len = b->len[i];
+    const uint32_t ls = b->line_start[i], le = b->len[i] ? b->line_start[i + 1] : ls;
+    if (first_line) *first_line = ls;
+    if (line_count) *line_count = le - ls;
+    return OL_OK;
+}
+
+extern "C" ol_status ol_batch_build_trees(ol_ctx *ctx, ol_batch *b) {
+    if (!ctx || !b || b->ctx != ctx) return OL_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    ol_tree *t = nullptr;
+    ol_status s = ol_tree_build_reusing(ctx, b->doc, b->tree, 0, &t);  // any depth: each document is checked alone
+    b->tree = nullptr;
+    if (s != OL_OK) return s;
+    b->tree = t;
+    const uint32_t L = b->doc->line_count;
+    uint32_t *p = (uint32_t *)t->parent_buf.ptr, *e = (uint32_t *)t->end_buf.ptr, *fc = (uint32_t *)t->fc_buf.ptr,
+             *ns = (uint32_t *)t->ns_buf.ptr;
+    cudaError_t ce = launch_batch_tree_fixup(b->d_line_start, b->n, L, b->doc->kinds, p, e, fc, p, e, fc, ns, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+    return ctx_cuda(ctx, ce, "batch trees");
+}
+
+// Lines of document i: offsets relative to the document, kinds, and tree links
+// as line indices within the document (NONE stays NONE). Any output may be
+// NULL; cap must be at least the document's line count.
+extern "C" ol_status ol_batch_read_doc(ol_ctx *ctx, const ol_batch *b, uint32_t i, uint32_t *offsets, uint8_t *kinds,
+                                       uint32_t *parent, uint32_t *subtree_end, uint32_t *first_child,
+                                       uint32_t *next_sibling, uint64_t cap) {
+    if (!ctx || !b || i >= b->n) return OL_ERR_INVALID_ARG;
+    uint64_t ls, lc;
+    ol_batch_doc_info(b, i, nullptr, nullptr, &ls, &lc);
+    if (cap < lc) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "output capacity is smaller than the document's line count");
+    if (lc == 0) return OL_OK;
+    if ((parent || subtree_end || first_child || next_sibling) && !b->tree)
+        return ctx_fail(ctx, OL_ERR_INVALID_ARG, "the batch's trees are not built");
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = cudaSuccess;
+    struct Part {
+        void *dst;
+        const void *src;
+        size_t elem;
+        bool rebase;    // subtract the document's first line / byte
+    } parts[6] = {
+        {offsets, b->doc->offsets, 4, true},
+        {kinds, b->doc->kinds, 1, false},
+        {parent, b->tree ? b->tree->parent_buf.ptr : nullptr, 4, true},
+        {subtree_end, b->tree ? b->tree->end_buf.ptr : nullptr, 4, true},
+        {first_child, b->tree ? b->tree->fc_buf.ptr : nullptr, 4, true},
+        {next_sibling, b->tree ? b->tree->ns_buf.ptr : nullptr, 4, true},
+    };
+    for (auto &p : parts)
+        if (p.dst && e == cudaSuccess)
+            e = cudaMemcpyAsync(p.dst, (const uint8_t *)p.src + ls * p.elem, lc * p.elem, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "batch read");
+    if (offsets)
+        for (uint64_t j = 0; j < lc; j++) offsets[j] -= (uint32_t)b->start[i];
+    for (int k = 2; k < 6; k++) {
+        uint32_t *a = (uint32_t *)parts[k].dst;
+        if (!a) continue;
+        for (uint64_t j = 0; j < lc; j++)
+            if (a[j] != NONE) a[j] -= (uint32_t)ls;
+    }
+    return OL_OK;
+}
+
+// Dictionary search over every document of the batch at once. Hits are
+// {pattern, offset in the batch text} in (pattern, offset) order, which is
+// (pattern, document, offset) order; no hit crosses a document boundary.
+// counts and *total_hits are host outputs, d_hits device memory.
+extern "C" ol_status ol_batch_search_many(ol_ctx *ctx, const ol_batch *b, const ol_patset *set, uint64_t max_hits,
+                                          uint32_t heavy_min_hits, uint32_t *counts, uint64_t *total_hits,
+                                          ol_hit *d_hits) {
+    if (!ctx || !b || !set || !counts || !total_hits || (max_hits && !d_hits)) return OL_ERR_INVALID_ARG;
+    if (b->ctx != ctx) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "batch belongs to another context");
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return many_run(ctx, b->doc, set, max_hits, heavy_min_hits, counts, total_hits, nullptr, d_hits, b->seg_start,
+                    b->seg_end, b->n);
+}

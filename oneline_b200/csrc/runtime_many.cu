@@ -209,12 +209,13 @@ extern "C" void ol_patset_free(ol_patset *s) {
 extern "C" uint32_t ol_patset_len(const ol_patset *s) { return s ? s->n_ids : 0; }
 extern "C" uint32_t ol_patset_unique(const ol_patset *s) { return s ? s->n_u : 0; }
 
-namespace {
 
 // The whole search; hits go to d_hits (capacity max_hits) when given, else to
 // host_hits through ctx->dict_hits. counts (n_ids) and *total are host outputs.
-ol_status many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits, uint32_t heavy_min_hits,
-                   uint32_t *counts, uint64_t *total, ol_hit *host_hits, ol_hit *d_hits) {
+// seg_start/seg_end (device, n_seg): batches, whose hits stay inside a document.
+ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits, uint32_t heavy_min_hits,
+                       uint32_t *counts, uint64_t *total, ol_hit *host_hits, ol_hit *d_hits,
+                       const unsigned long long *seg_start, const unsigned long long *seg_end, uint32_t n_seg) {
     cudaStream_t st = ctx->stream;
     const uint32_t n = set->n_ids, U = set->n_u;
     const uint64_t N = d->text_len;
@@ -274,6 +275,9 @@ ol_status many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t 
     ma.count_only = 1;
     ma.counts = m.sample_counts;
     ma.error = m.error;
+    ma.seg_start = seg_start;
+    ma.seg_end = seg_end;
+    ma.n_seg = n_seg;
     e = cudaMemsetAsync(m.sample_counts, 0, (size_t)U * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(m.light_n, 0, 16, st);
     if (e == cudaSuccess) e = launch_dict_match(ma, ctx->sm_count, st);
@@ -410,15 +414,13 @@ ol_status many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t 
     return OL_OK;
 }
 
-}  // namespace
-
 extern "C" ol_status ol_search_many(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits,
                                     uint32_t *counts, uint64_t *total_hits, ol_hit *hits) {
     if (!ctx || !d || !set || !counts || !total_hits || (max_hits && !hits)) return OL_ERR_INVALID_ARG;
     if (set->ctx != ctx) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "pattern set belongs to another context");
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
-    return many_run(ctx, d, set, max_hits, 0, counts, total_hits, hits, nullptr);
+    return many_run(ctx, d, set, max_hits, 0, counts, total_hits, hits, nullptr, nullptr, nullptr, 0);
 }
 
 extern "C" ol_status ol_search_many_device(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits,
@@ -428,5 +430,5 @@ extern "C" ol_status ol_search_many_device(ol_ctx *ctx, const ol_doc *d, const o
     if (set->ctx != ctx) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "pattern set belongs to another context");
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
-    return many_run(ctx, d, set, max_hits, heavy_min_hits, counts, total_hits, nullptr, d_hits);
+    return many_run(ctx, d, set, max_hits, heavy_min_hits, counts, total_hits, nullptr, d_hits, nullptr, nullptr, 0);
 }

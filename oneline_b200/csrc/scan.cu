@@ -94,7 +94,7 @@ cudaError_t launch_scan_columns(const uint32_t *in, uint32_t *out, uint32_t *tot
                                 uint32_t ld, cudaStream_t st) {
     if (rows == 0 || cols == 0) return cudaSuccess;
     dim3 grid((rows + SC_CHUNK - 1) / SC_CHUNK, cols);
-    scan_columns_kernel<<<grid, SC_THREADS, 0, st>>>(in, out, totals, rows, ld);
+    scan_columns_kernel<<<grid, SC_THREADS, 0, st>>>(in, out, totals, rows, ld); OL_LAUNCHED();
     return cudaGetLastError();
 }
 

@@ -281,10 +281,10 @@ __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) 
 
 cudaError_t launch_search(const SearchArgs &a, cudaStream_t st) {
     if (a.n_tiles == 0 || a.np == 0) return cudaSuccess;
-    search_count_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a);
+    search_count_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
     cudaError_t e = launch_scan_columns(a.counts, a.bases, a.totals, a.n_tiles, a.np, a.ld, st);
     if (e != cudaSuccess) return e;
-    search_write_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a);
+    search_write_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
     return cudaGetLastError();
 }
 

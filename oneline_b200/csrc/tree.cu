@@ -338,9 +338,9 @@ cudaError_t launch_tree_fast(const TreeArgs &a, cudaStream_t st) {
             e = cudaFuncSetAttribute(tree_resolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    tree_summary_kernel<<<a.n_tiles, TR_THREADS, smem, st>>>(a);
-    tree_scan_kernel<<<a.levels, 1024, 0, st>>>(a);
-    tree_resolve_kernel<<<a.n_tiles, TR_THREADS, smem, st>>>(a);
+    tree_summary_kernel<<<a.n_tiles, TR_THREADS, smem, st>>>(a); OL_LAUNCHED();
+    tree_scan_kernel<<<a.levels, 1024, 0, st>>>(a); OL_LAUNCHED();
+    tree_resolve_kernel<<<a.n_tiles, TR_THREADS, smem, st>>>(a); OL_LAUNCHED();
     return cudaGetLastError();
 }
 
@@ -444,10 +444,10 @@ cudaError_t launch_tree_deep(const TreeDeepArgs &a, cudaStream_t st) {
     if (a.L == 0) return cudaSuccess;
     for (uint32_t l = 1; l < a.n_levels; l++) {
         uint32_t m = a.level_len[l];
-        min_level_kernel<<<(m + 255) / 256, 256, 0, st>>>(a.levels[l - 1], a.level_len[l - 1], a.levels[l], m);
+        min_level_kernel<<<(m + 255) / 256, 256, 0, st>>>(a.levels[l - 1], a.level_len[l - 1], a.levels[l], m); OL_LAUNCHED();
     }
-    deep_links_kernel<<<(a.L + 255) / 256, 256, 0, st>>>(a);
-    deep_children_kernel<<<(a.L + 255) / 256, 256, 0, st>>>(a);
+    deep_links_kernel<<<(a.L + 255) / 256, 256, 0, st>>>(a); OL_LAUNCHED();
+    deep_children_kernel<<<(a.L + 255) / 256, 256, 0, st>>>(a); OL_LAUNCHED();
     return cudaGetLastError();
 }
 

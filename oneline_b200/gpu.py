@@ -217,6 +217,43 @@ class GpuPatternSet:
             pass
 
 
+class GpuBatch:
+    """Many documents resident as one text (no reference counterpart: per document
+    the results equal upload / build_tree / search_many on that document alone)."""
+
+    def __init__(self, parser: "GpuParser", handle: int):
+        self._parser = parser
+        self._h = handle
+        parser._children.add(self)
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def __len__(self) -> int:
+        return int(_lib.load().ol_batch_docs(self._h))
+
+    def text_len(self) -> int:
+        return int(_lib.load().ol_batch_text_len(self._h))
+
+    def doc_info(self, i: int) -> tuple[int, int, int, int]:
+        """(text_start, text_len, first_line, line_count) of document i."""
+        v = [ctypes.c_uint64() for _ in range(4)]
+        check(_lib.load().ol_batch_doc_info(self._h, i, *[ctypes.byref(x) for x in v]))
+        return tuple(int(x.value) for x in v)
+
+    def free(self) -> None:
+        if self._h and self._parser._ctx:
+            _lib.load().ol_batch_free(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 class GpuParser:
     """Parser and search engine on one CUDA device (parser.rs:8-142)."""
 
@@ -489,4 +526,50 @@ class GpuParser:
         check(_lib.load().ol_search_many_device(self._ctx, doc.handle, pattern_set.handle, int(max_hits),
                                                 int(heavy_min_hits), counts.ctypes.data, ctypes.byref(total),
                                                 d_hits), self._ctx)
+        return counts, int(total.value)
+
+    # -------------------------------------------------------------- batches
+
+    def upload_batch(self, docs) -> GpuBatch:
+        """Uploads and parses many documents as one batch; `docs` is a list of
+        byte strings, or (data, offsets) with document i = data[offsets[i]:offsets[i+1]]."""
+        if isinstance(docs, tuple):
+            data, offs = docs
+            data = np.ascontiguousarray(np.frombuffer(data, np.uint8) if isinstance(data, (bytes, bytearray)) else data,
+                                        dtype=np.uint8)
+            offs = np.ascontiguousarray(offs, dtype=np.uint64)
+        else:
+            parts = [d.encode("utf-8") if isinstance(d, str) else bytes(d) for d in docs]
+            data = np.frombuffer(b"".join(parts), np.uint8) if parts and any(parts) else np.zeros(1, np.uint8)
+            offs = np.zeros(len(parts) + 1, np.uint64)
+            offs[1:] = np.cumsum([len(p) for p in parts])
+        h = ctypes.c_void_p()
+        check(_lib.load().ol_batch_upload(self._ctx, data.ctypes.data, offs.ctypes.data, offs.size - 1,
+                                          ctypes.byref(h)), self._ctx)
+        return GpuBatch(self, h.value)
+
+    def build_batch_trees(self, batch: GpuBatch) -> None:
+        check(_lib.load().ol_batch_build_trees(self._ctx, batch.handle), self._ctx)
+
+    def read_batch_doc(self, batch: GpuBatch, i: int, *, tree: bool = True) -> dict:
+        """Document i's offsets, kinds and (when built) tree links, all relative to the document."""
+        _, _, _, n = batch.doc_info(i)
+        out = {"offsets": np.zeros(max(n, 1), np.uint32), "kinds": np.zeros(max(n, 1), np.uint8)}
+        names = ("parent", "subtree_end", "first_child", "next_sibling")
+        for k in names:
+            out[k] = np.zeros(max(n, 1), np.uint32) if tree else None
+        ptr = lambda a: a.ctypes.data if a is not None else None  # noqa: E731
+        check(_lib.load().ol_batch_read_doc(self._ctx, batch.handle, i, ptr(out["offsets"]), ptr(out["kinds"]),
+                                            *[ptr(out[k]) for k in names], n), self._ctx)
+        return {k: (v[:n] if v is not None else None) for k, v in out.items()}
+
+    def batch_search_many(self, batch: GpuBatch, pattern_set: GpuPatternSet, d_hits: int, max_hits: int, *,
+                          heavy_min_hits: int = 0) -> tuple[np.ndarray, int]:
+        """Dictionary search of every document of the batch; hits (device, at d_hits) hold
+        offsets in the batch text, in (pattern, document, offset) order. Returns (counts, total)."""
+        counts = np.zeros(len(pattern_set), np.uint32)
+        total = ctypes.c_uint64()
+        check(_lib.load().ol_batch_search_many(self._ctx, batch.handle, pattern_set.handle, int(max_hits),
+                                               int(heavy_min_hits), counts.ctypes.data, ctypes.byref(total),
+                                               d_hits), self._ctx)
         return counts, int(total.value)
