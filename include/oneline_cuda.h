@@ -231,6 +231,42 @@ ol_status ol_batch_read_doc(ol_ctx *ctx, const ol_batch *batch, uint32_t i, uint
 ol_status ol_batch_search_many(ol_ctx *ctx, const ol_batch *batch, const ol_patset *set, uint64_t max_hits,
                                uint32_t heavy_min_hits, uint32_t *counts, uint64_t *total_hits, ol_hit *d_hits);
 
+/* ---- serving. No counterpart in the reference (one blocking call per
+ *      document). A server owns `workers` threads, each with its own context
+ *      and stream: queued requests start as soon as a worker frees up and their
+ *      kernels overlap on the device. Parsed documents (text, line arrays, tree
+ *      links) stay resident in a store of at most store_budget bytes: the least
+ *      recently used idle documents are evicted to make room, and a document
+ *      that does not fit beside the ones in use is refused (OL_ERR_ADMISSION).
+ *      A search names a resident document (OL_ERR_NOT_FOUND once evicted) and
+ *      searches it for 1..OL_MAX_DICT_PATTERNS set patterns; each worker keeps
+ *      up to max_hits hits in device memory. Results carry a digest of the
+ *      outputs, computed on the device, to compare runs. */
+typedef struct ol_server ol_server;
+typedef struct ol_request_result {
+    uint64_t id;
+    uint32_t kind;        /* 0 parse, 1 search */
+    ol_status status;
+    uint32_t worker;
+    uint32_t pad;
+    uint64_t doc_id;      /* parse: the new resident document; search: the document searched */
+    uint64_t line_count;  /* parse */
+    uint64_t total_hits;  /* search */
+    uint64_t digest;      /* parse: offsets, kinds, parent, subtree_end, first_child, next_sibling; search: counts, hits */
+    uint64_t submit_ns, start_ns, end_ns;  /* steady clock */
+} ol_request_result;
+ol_status ol_server_create(int32_t device, uint32_t workers, uint64_t store_budget, uint64_t max_hits, ol_server **out);
+/* Finishes the queued requests, then frees every resident document. */
+void ol_server_destroy(ol_server *server);
+/* The text must stay valid until the request completes. */
+ol_status ol_server_submit_parse(ol_server *server, const uint8_t *text, uint64_t len, uint64_t *request_id);
+ol_status ol_server_submit_search(ol_server *server, uint64_t doc_id, const uint8_t *const *patterns,
+                                  const uint32_t *lens, uint32_t n, uint64_t *request_id);
+/* Blocks until the request is done and returns its result (once). */
+ol_status ol_server_wait(ol_server *server, uint64_t request_id, ol_request_result *out);
+ol_status ol_server_stats(ol_server *server, uint64_t *resident_docs, uint64_t *resident_bytes, uint64_t *evictions,
+                          uint64_t *refusals);
+
 /* ---- substring search that allocates nothing. No counterpart in the
  *      reference: an addition for callers that cannot call cudaMalloc, such as a
  *      serving process whose own allocator reserved the GPU's memory up front, or

@@ -213,6 +213,10 @@ struct DictEmitArgs {
 };
 cudaError_t launch_dict_ids(const DictEmitArgs &a, cudaStream_t st);
 
+// Digests (digest.cu): *out += sum of per-element hashes of a[0..n).
+cudaError_t launch_digest_u32(const uint32_t *a, uint64_t n, uint32_t seed, unsigned long long *out, cudaStream_t st);
+cudaError_t launch_digest_u8(const uint8_t *a, uint64_t n, uint32_t seed, unsigned long long *out, cudaStream_t st);
+
 // Batches (batch.cu).
 cudaError_t launch_batch_line_starts(const uint32_t *offsets, uint32_t L, const unsigned long long *seg_start, uint32_t n,
                                      uint32_t *line_start, cudaStream_t st);

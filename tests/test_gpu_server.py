@@ -1,0 +1,80 @@
+"""The serving loop: every result equals the oracle's and is the same when the
+request runs alone and when it runs among others; the HBM-budgeted store
+evicts idle documents and refuses what cannot fit."""
+import numpy as np
+import pytest
+
+import oracle
+from oneline_b200 import datagen
+from oneline_b200.serving import GpuServer, parse_digest, search_digest
+
+pytestmark = pytest.mark.gpu
+
+OL_ERR_ADMISSION, OL_ERR_NOT_FOUND = 6, 9
+
+
+def workload():
+    texts = []
+    for i, size in enumerate([1 << 10, 5000, 64 << 10, 300 << 10, 1 << 20, 3 << 20, 777, 2 << 20]):
+        texts.append(datagen.generate(datagen.ALL_PROFILES[i % len(datagen.ALL_PROFILES)], size, 50 + i))
+    searches = []
+    for i, t in enumerate(texts):
+        arr = np.frombuffer(t, np.uint8)
+        for n in (1, 7, 64):
+            searches.append((i, datagen.patterns_dictionary(arr, 60 + i * 3 + n, n=n)))
+    return texts, searches
+
+
+def oracle_digests(texts, searches):
+    parse, search = [], []
+    for t in texts:
+        offs, nodes = oracle.parse(t)
+        tr = oracle.full_tree(nodes)
+        parse.append(parse_digest(offs, nodes["kind"].astype(np.uint8), tr["parent"], tr["subtree_end"],
+                                  tr["first_child"], tr["next_sibling"]))
+    for i, pats in searches:
+        counts, hp, ho = oracle.find_many(texts[i], pats)
+        search.append(search_digest(counts, hp, ho, len(hp)))
+    return parse, search
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix():
+    texts, searches = workload()
+    want_parse, want_search = oracle_digests(texts, searches)
+    with GpuServer(workers=1, store_budget=1 << 30) as alone:
+        ap = [alone.wait(alone.submit_parse(t)) for t in texts]
+        asr = [alone.wait(alone.submit_search(ap[i].doc_id, pats)) for i, pats in searches]
+    with GpuServer(workers=6, store_budget=1 << 30) as mix:
+        ids = [mix.submit_parse(t) for t in texts]
+        mp = [mix.wait(r) for r in ids]
+        # searches interleaved with more parse requests of the same texts
+        sids, extra = [], []
+        for k, (i, pats) in enumerate(searches):
+            sids.append(mix.submit_search(mp[i].doc_id, pats))
+            if k % 3 == 0:
+                extra.append((k % len(texts), mix.submit_parse(texts[k % len(texts)])))
+        ms = [mix.wait(r) for r in sids]
+        me = [(i, mix.wait(r)) for i, r in extra]
+        assert len({r.worker for r in mp + ms}) > 1  # the work was spread over workers
+    for r in ap + asr + mp + ms:
+        assert r.status == 0
+    assert [r.digest for r in ap] == want_parse == [r.digest for r in mp]
+    assert [r.digest for r in asr] == want_search == [r.digest for r in ms]
+    for i, r in me:
+        assert r.status == 0 and r.digest == want_parse[i]
+
+
+def test_store_budget_evicts_and_refuses():
+    t = datagen.corpus(1 << 20, 9).tobytes()
+    big = datagen.corpus(24 << 20, 10).tobytes()
+    with GpuServer(workers=2, store_budget=8 << 20) as s:
+        docs = [s.wait(s.submit_parse(t)) for _ in range(12)]
+        assert all(r.status == 0 for r in docs)
+        st = s.stats()
+        assert st["evictions"] > 0 and st["resident_bytes"] <= 8 << 20
+        gone = s.wait(s.submit_search(docs[0].doc_id, [b"||||"]))
+        assert gone.status == OL_ERR_NOT_FOUND
+        kept = s.wait(s.submit_search(docs[-1].doc_id, [b"||||"]))
+        assert kept.status == 0 and kept.total_hits > 0
+        r = s.wait(s.submit_parse(big))
+        assert r.status == OL_ERR_ADMISSION and s.stats()["refusals"] == 1
