@@ -50,7 +50,7 @@ def hbm_peak():
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--bytes", type=int, default=1 << 30, help="document size (default 1 GiB)")
@@ -60,20 +60,49 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-launches", action="store_true",
                     help="one short run for an ncu launch list (no e2e, no CPU leg)")
+    ap.add_argument("--workload", default="parse_search", choices=["parse_search", "dictionary", "batch", "serve"],
+                    help="parse_search: 1 GiB parse + 8-pattern search (the headline); dictionary: 1 GiB x "
+                         "10,000 patterns; batch: 10,000 uneven documents, batched vs one call per document; "
+                         "serve: open-loop Poisson parse/search requests, concurrent workers vs one")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the serve workload's arrival stream")
+    ap.add_argument("--serve-workers", type=int, default=8)
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean arrivals per second")
     return ap.parse_args()
 
 
 # ------------------------------------------------------------------ helpers
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 2 ms from a thread (read-only queries), plus a
+    nvidia-smi log (100 ms) kept in gpurun_out/ for the record."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.samples = []
+        self.max_mhz = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
 
+    def _poll(self):
+        import pynvml
+
+        h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+            r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.samples.append((sm, r))
+            self._stop.wait(0.002)
+
     def __enter__(self):
+        import threading
+
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -85,24 +114,43 @@ class ClockSampler:
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        self._stop = threading.Event()
+        self._thread = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self._thread = threading.Thread(target=self._poll, daemon=True)
+            self._thread.start()
+        except Exception:
+            self._thread = None
         return self
 
     def __exit__(self, *a):
+        self._stop.set()
+        if self._thread:
+            self._thread.join()
         if self.proc:
             self.proc.terminate()
             self.proc.wait()
             self.f.close()
 
     def summary(self):
-        try:
+        import pynvml
+
+        if self.samples:
+            names = [n for n, attr in self.REASONS if any(r & getattr(pynvml, attr) for _, r in self.samples)]
+            return {"sm_mhz": statistics.median(s for s, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                    "reasons": names, "samples": len(self.samples), "source": "NVML every 2 ms"}
+        try:  # nvidia-smi log only
             rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
             rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
             sm = [float(r[1]) for r in rows]
             mx = float(rows[0][2]) if rows else None
-            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            names = [n for n, _ in self.REASONS]
             reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
             return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
-                    "samples": len(rows)}
+                    "samples": len(rows), "source": "nvidia-smi every 100 ms"}
         except Exception as e:  # nvidia-smi missing
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": str(e)[:80]}
 
@@ -282,8 +330,6 @@ def run_ours(args, world, rank, local):
         enqueue_tree()
         enqueue_search()
 
-    # parse: count, scan, tiles, fix-up; tree: summary, scan, resolve; search: count, scan, write per 8 patterns
-    launches_per_step = 4 + 3 + 3 * ((n_p + 7) // 8)
     if args.profile_launches:
         for _ in range(args.warmup + args.steps):
             step()
@@ -318,6 +364,7 @@ def run_ours(args, world, rank, local):
     barrier(world)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = L.ol_launch_count()
     with ClockSampler(local) as clocks:
         with torch.cuda.stream(stream):
             ev0.record()
@@ -326,6 +373,7 @@ def run_ours(args, world, rank, local):
         with torch.cuda.stream(stream):
             ev1.record()
         ev1.synchronize()
+    launches = L.ol_launch_count() - l0
     torch.cuda.synchronize()
     barrier(world)
     ms = ev0.elapsed_time(ev1) / args.steps
@@ -341,13 +389,12 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = hbm_peak()
     hits = sum(totals)
     # algorithmic bytes: text read once per launch + every output byte once
-    groups = {"parse_tiles_kernel": (t_parse, N + 6 * lines),
-              "tree_forward+backward": (t_tree, 2 * lines + 5 * lines + 3 * lines + 16 * lines),
-              "search_kernel<8>": (t_search, N + 4 * hits)}
+    groups = {"parse pass (newline_count, scan, parse_tiles, fixup)": (t_parse, N + 6 * lines),
+              "tree pass (summary, scan, resolve)": (t_tree, 2 * lines + 16 * lines),
+              "8-pattern search pass (search_count, scan, search_write)": (t_search, N + 4 * hits)}
     dom = max(groups, key=lambda k: groups[k][0])
-    launches = 1
-    t_launch = groups[dom][0] / launches
-    alg = groups[dom][1] / launches
+    t_launch = groups[dom][0]
+    alg = groups[dom][1]
     achieved = alg / (t_launch * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
@@ -406,9 +453,358 @@ def run_ours(args, world, rank, local):
                 "vs_baseline": None, "dtype": "u8", "data": "synthetic",
                 "config": {**workload_config(args, N, pats, lines), "hits": totals},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches_per_step * args.steps, "clocks": clocks.summary(),
+                "gpu_launches": int(launches), "clocks": clocks.summary(),
                 "device": p.adapter_name()}
         print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------ dictionary
+
+def run_dictionary(args, world, rank, local):
+    """1 GiB synthetic document (seed 2) against 10,000 patterns of 4..64 B: every
+    (pattern id, offset) hit in (pattern, offset) order, left in HBM (value) or
+    downloaded (e2e)."""
+    import torch
+
+    from oneline_b200 import GpuParser, _lib, datagen
+
+    L = _lib.load()
+    seed = 2 + rank
+    text = datagen.corpus(args.bytes, seed)
+    pats = datagen.patterns_dictionary(text, seed, n=10_000)
+    N = text.size
+    torch.cuda.set_device(local)
+    p = GpuParser(local)
+    host = torch.empty(N, dtype=torch.uint8, pin_memory=True)
+    host.numpy()[:] = text
+    doc = p.upload(host.numpy())
+    ps = p.compile_patterns(doc, pats, max_patterns=None)
+    counts, total = p.search_many_device(doc, ps, 0, 0)
+    hits = torch.empty(2 * max(total, 1), dtype=torch.int32, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(L.ol_ctx_stream(p.ctx), device=f"cuda:{local}")
+
+    def step():
+        c, t = p.search_many_device(doc, ps, hits.data_ptr(), total)
+        assert t == total
+
+    for _ in range(args.warmup):
+        step()
+    p.sync()
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = L.ol_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            ev0.record()
+        for _ in range(args.steps):
+            step()
+        with torch.cuda.stream(stream):
+            ev1.record()
+        ev1.synchronize()
+    launches = L.ol_launch_count() - l0
+    ms = allreduce_max(ev0.elapsed_time(ev1) / args.steps, world)
+    bytes_all = allreduce_sum(float(N), world)
+    value = bytes_all / (ms * 1e-3) / 1e9
+    peak, peak_kind = hbm_peak()
+    alg = N + 8 * total  # text once + every ManyHit {pattern u32, offset u32} once
+    achieved = alg / (ms * 1e-3) / 1e9
+
+    e2e = None
+    if args.e2e_steps > 0:
+        out_h = torch.empty(2 * max(total, 1), dtype=torch.int32, pin_memory=True)
+        cnt_h = np.zeros(len(pats), np.uint32)
+        tot_h = ctypes.c_uint64()
+
+        def e2e_step():
+            h = ctypes.c_void_p()
+            chk = lambda s: (_ for _ in ()).throw(RuntimeError(L.ol_last_error(p.ctx).decode())) if s else None  # noqa
+            chk(L.ol_doc_upload(p.ctx, host.data_ptr(), N, ctypes.byref(h)))
+            chk(L.ol_search_many(p.ctx, h.value, ps.handle, total, cnt_h.ctypes.data, ctypes.byref(tot_h),
+                                 out_h.data_ptr()))
+            L.ol_doc_free(h.value)
+
+        e2e_step()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        dt = allreduce_max((time.perf_counter() - t0) / args.e2e_steps, world)
+        e2e = {"value": round(bytes_all / dt / 1e9, 4), "unit": "GB/s", "ms_per_step": round(dt * 1e3, 2),
+               "h2d_bytes_per_step": int(N), "d2h_bytes_per_step": int(8 * total + 4 * len(pats) + 8),
+               "timing": "host wall clock around blocking C-ABI calls, max over ranks",
+               "path": "ol_doc_upload (pinned text) + ol_search_many (counts and every hit to pinned host memory)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        import oracle
+
+        n = min(N, 32 << 20)
+        sample = np.ascontiguousarray(text[:n])
+        many = oracle.CpuBaseline().many(pats)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            many.find_all_par(sample)
+            ts.append(time.perf_counter() - t0)
+        t = statistics.median(ts[1:])
+        cpu = {"value": round(n / t / 1e9, 4), "unit": "GB/s", "cores": many.threads, "kind": "port",
+               "sample": f"first {n} bytes of the same document x the same 10,000 patterns: Aho-Corasick DFA "
+                         f"(byte classes), all hits sorted by (pattern, offset); median of 2 after 1 warm-up",
+               "dfa_states": int(many.states)}
+
+    if rank == 0:
+        line = {"metric": "dictionary search GB/s vs HBM peak", "value": round(value, 3), "unit": "GB/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic",
+                "config": {"workload": f"{N}-byte synthetic oneline document (seed {seed}) x 10,000-pattern "
+                                       f"dictionary (4..64 B, 60% sampled from the text): every (pattern, offset)",
+                           "text_bytes": int(N), "patterns": len(pats), "unique_patterns": ps.unique(),
+                           "total_hits": int(total), "hit_bytes": int(8 * total),
+                           "l2": "inputs and outputs larger than L2 (no flush needed)",
+                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                "roofline": {"bound": "hbm", "kernel": "dictionary pass (match, rank, sort, emit)",
+                             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
+                             "alg_bytes_per_launch": int(alg), "ms_per_launch": round(ms, 3)},
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks.summary(),
+                "device": p.adapter_name()}
+        print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- batch
+
+def run_batch(args, world, rank, local):
+    """10,000 documents (seeds 3..10002, log-normal sizes, median 16 KiB, sigma 1.5,
+    256 B..64 MiB): full parse, tree links and a 1,000-pattern dictionary search of
+    every document, batched (one upload, one parse, one tree build, one search) vs
+    one call per document, both end to end from host memory."""
+    import torch
+
+    from oneline_b200 import GpuParser, _lib, datagen
+
+    L = _lib.load()
+    n_docs = 10_000
+    sizes = datagen.lognormal_sizes(3, n_docs, 16384.0, 1.5, 256, 64 << 20)
+    docs = [datagen.corpus(int(sz), 3 + i) for i, sz in enumerate(sizes)]
+    offs = np.zeros(n_docs + 1, np.uint64)
+    offs[1:] = np.cumsum(sizes)
+    data_np = np.concatenate(docs)
+    total_bytes = int(offs[-1])
+    dict_text = datagen.corpus(1 << 30, 2)
+    pats = datagen.patterns_dictionary(dict_text, 2, n=10_000)[:1000]
+    del dict_text
+    torch.cuda.set_device(local)
+    p = GpuParser(local)
+    data = torch.empty(total_bytes, dtype=torch.uint8, pin_memory=True)
+    data.numpy()[:] = data_np
+    ps = p.compile_patterns(None, pats)
+    cnt = np.zeros(len(pats), np.uint32)
+    tot = ctypes.c_uint64()
+
+    def chk(s):
+        if s != 0:
+            raise RuntimeError(L.ol_last_error(p.ctx).decode())
+
+    # output room: the hits of the batched pass (same total as the per-document calls)
+    b0 = p.upload_batch((data.numpy(), offs))
+    _, total = p.batch_search_many(b0, ps, 0, 0)
+    b0.free()
+    hits = torch.empty(2 * max(total, 1), dtype=torch.int32, device=f"cuda:{local}")
+
+    def batched():
+        h = ctypes.c_void_p()
+        chk(L.ol_batch_upload(p.ctx, data.data_ptr(), offs.ctypes.data, n_docs, ctypes.byref(h)))
+        chk(L.ol_batch_build_trees(p.ctx, h.value))
+        chk(L.ol_batch_search_many(p.ctx, h.value, ps.handle, total, 0, cnt.ctypes.data, ctypes.byref(tot),
+                                   hits.data_ptr()))
+        L.ol_batch_free(h.value)
+        return int(tot.value)
+
+    def plain():
+        got = 0
+        base = data.data_ptr()
+        for i in range(n_docs):
+            h = ctypes.c_void_p()
+            t = ctypes.c_void_p()
+            chk(L.ol_doc_upload(p.ctx, base + int(offs[i]), int(sizes[i]), ctypes.byref(h)))
+            chk(L.ol_tree_build(p.ctx, h.value, 0, ctypes.byref(t)))
+            chk(L.ol_search_many_device(p.ctx, h.value, ps.handle, total - got, 0, cnt.ctypes.data, ctypes.byref(tot),
+                                        hits.data_ptr() + 8 * got))
+            got += int(tot.value)
+            L.ol_tree_free(t.value)
+            L.ol_doc_free(h.value)
+        return got
+
+    for _ in range(args.warmup):
+        batched()
+    p.sync()
+    barrier(world)
+    l0 = L.ol_launch_count()
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            got = batched()
+        p.sync()
+        dt = (time.perf_counter() - t0) / args.steps
+    launches = L.ol_launch_count() - l0
+    assert got == total
+    dt = allreduce_max(dt, world)
+    t0 = time.perf_counter()
+    got_plain = plain()
+    p.sync()
+    dt_plain = allreduce_max(time.perf_counter() - t0, world)
+    assert got_plain == total, (got_plain, total)
+    bytes_all = allreduce_sum(float(total_bytes), world)
+    value = bytes_all / dt / 1e9
+    if rank == 0:
+        plain_v = bytes_all / dt_plain / 1e9
+        line = {"metric": "batched parse+dictionary GB/s vs one call per document", "value": round(value, 3),
+                "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(dt * 1e3, 2), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u8", "data": "synthetic",
+                "config": {"workload": f"{n_docs} documents (seeds 3..{2 + n_docs}, log-normal sizes median 16 KiB, "
+                                       f"sigma 1.5, 256 B..64 MiB, {total_bytes} bytes): parse + tree links + "
+                                       f"1,000-pattern dictionary search of every document",
+                           "docs": n_docs, "text_bytes": total_bytes, "patterns": len(pats), "total_hits": int(total),
+                           "l2": "inputs larger than L2", "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                "plain": {"value": round(plain_v, 4), "unit": "GB/s", "ms_per_step": round(dt_plain * 1e3, 1),
+                          "path": "per document: ol_doc_upload + ol_tree_build + ol_search_many_device"},
+                "speedup_vs_plain": round(value / plain_v, 2),
+                "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": total_bytes,
+                        "d2h_bytes_per_step": 4 * len(pats) + 8,
+                        "timing": "host wall clock around the blocking batch calls (the value itself)",
+                        "path": "ol_batch_upload (pinned) + ol_batch_build_trees + ol_batch_search_many (hits in HBM)"},
+                "gpu_launches": int(launches), "clocks": clocks.summary(), "device": p.adapter_name()}
+        print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- serve
+
+def serve_stream(seconds: float, seed: int = 4, rate: float = 2000.0):
+    """The request stream: Poisson arrivals at 2,000 req/s; 30% parse requests
+    (log-normal sizes, median 64 KiB, sigma 2, 1 KiB..64 MiB, cut from a seeded
+    corpus), 70% searches of 1..64 patterns (4..64 B) against resident documents."""
+    from oneline_b200 import datagen
+
+    n = int(rate * seconds)
+    t = datagen.poisson_arrivals(seed, n, rate)
+    rng = datagen.Rng(seed)
+    is_parse = np.array([rng.below(100) < 30 for _ in range(n)])
+    sizes = datagen.lognormal_sizes(seed, n, 65536.0, 2.0, 1024, 64 << 20)
+    base = datagen.corpus(256 << 20, seed)
+    pool = datagen.patterns_dictionary(base[: 64 << 20], seed, n=20_000)
+    reqs = []
+    for i in range(n):
+        if is_parse[i]:
+            size = int(sizes[i])
+            at = rng.below(base.size - size) if base.size > size else 0
+            reqs.append(("parse", float(t[i]), base[at: at + size]))
+        else:
+            k = 1 + rng.below(64)
+            first = rng.below(len(pool) - k)
+            reqs.append(("search", float(t[i]), pool[first: first + k], rng.below(1 << 30)))
+    return reqs, base
+
+
+def serve_run(reqs, workers: int, warm_docs):
+    """Plays the stream open-loop against a server; returns per-request latencies
+    and the bytes processed."""
+    import threading
+
+    from oneline_b200.serving import GpuServer
+
+    with GpuServer(workers=workers, store_budget=4 << 30, max_hits=1 << 22) as srv:
+        # warm-up outside the timed stream: resident documents to search, and
+        # every kernel launched once (the first launch of a kernel loads it)
+        ready = [srv.wait(r).doc_id for r in [srv.submit_parse(d) for d in warm_docs]]
+        sizes = {d: int(len(w)) for d, w in zip(ready, warm_docs)}
+        for r in [srv.submit_search(d, [b"||||", b"| @", b"abcd"][: 1 + d % 3]) for d in ready]:
+            srv.wait(r)
+        lock = threading.Lock()
+        pending = []  # (request id, kind, bytes, doc size for searches)
+        done = threading.Event()
+        results = []
+
+        def collect():
+            i = 0
+            while True:
+                with lock:
+                    item = pending[i] if i < len(pending) else None
+                if item is None:
+                    if done.is_set():
+                        with lock:
+                            if i >= len(pending):
+                                return
+                    time.sleep(0.0002)
+                    continue
+                rid, kind, nbytes = item
+                r = srv.wait(rid)
+                if kind == "parse" and r.status == 0:
+                    with lock:
+                        ready.append(r.doc_id)
+                        sizes[r.doc_id] = nbytes
+                results.append((kind, r.status, r.latency_ns, nbytes if kind == "parse" else sizes.get(r.doc_id, 0),
+                                r.start_ns, r.end_ns))
+                i += 1
+
+        col = threading.Thread(target=collect)
+        col.start()
+        t0 = time.perf_counter()
+        for req in reqs:
+            delay = t0 + req[1] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            if req[0] == "parse":
+                rid = srv.submit_parse(req[2])
+                with lock:
+                    pending.append((rid, "parse", int(req[2].size)))
+            else:
+                with lock:
+                    doc = ready[req[3] % len(ready)]
+                rid = srv.submit_search(doc, req[2])
+                with lock:
+                    pending.append((rid, "search", 0))
+        done.set()
+        col.join()
+        wall = time.perf_counter() - t0
+        stats = srv.stats()
+    return results, wall, stats
+
+
+def run_serve(args, world, rank, local):
+    if rank != 0:
+        return
+    from oneline_b200 import GpuParser, datagen
+
+    reqs, base = serve_stream(args.serve_seconds, rate=args.serve_rate)
+    warm = [base[i << 20: (i << 20) + (64 << 10)] for i in range(64)]
+    out = {}
+    for name, workers in (("served", args.serve_workers), ("plain", 1)):
+        with ClockSampler(local) as clocks:
+            res, wall, stats = serve_run(reqs, workers, warm)
+        ok = [r for r in res if r[1] == 0]
+        lat = np.array([r[2] for r in ok], np.float64) / 1e6
+        span = (max(r[5] for r in ok) - min(r[4] for r in ok)) / 1e9
+        nbytes = sum(r[3] for r in ok)
+        out[name] = {"workers": workers, "requests": len(res), "ok": len(ok),
+                     "refused": sum(1 for r in res if r[1] == 6), "not_found": sum(1 for r in res if r[1] == 9),
+                     "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                     "req_per_s": round(len(ok) / wall, 1), "gb_per_s": round(nbytes / span / 1e9, 3),
+                     "wall_s": round(wall, 2), "store": stats, "clocks": clocks.summary()}
+    sv, pl = out["served"], out["plain"]
+    line = {"metric": "served req/s at p99 vs per-request launches", "value": sv["req_per_s"], "unit": "req/s",
+            "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": round(sv["wall_s"] * 1e3, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": f"open-loop Poisson stream, {args.serve_rate:g} req/s for {args.serve_seconds} s: 30% parse "
+                                   "(log-normal 64 KiB median, sigma 2, 1 KiB..64 MiB), 70% search (1..64 patterns "
+                                   "of 4..64 B) against resident documents; 4 GiB store with HBM-budget admission",
+                       "requests": len(reqs), "parallelism": "single GPU"},
+            "served": sv, "plain": pl,
+            "p99_speedup_vs_plain": round(pl["p99_ms"] / max(sv["p99_ms"], 1e-9), 2),
+            "gbps_vs_plain": round(sv["gb_per_s"] / max(pl["gb_per_s"], 1e-9), 2),
+            "device": GpuParser(local).adapter_name()}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -417,6 +813,12 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "dictionary":
+            run_dictionary(args, world, rank, local)
+        elif args.workload == "batch":
+            run_batch(args, world, rank, local)
+        elif args.workload == "serve":
+            run_serve(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
