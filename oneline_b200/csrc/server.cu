@@ -295,6 +295,19 @@ extern "C" ol_status ol_server_create(int32_t device, uint32_t workers, uint64_t
         }
         s->ctxs.push_back(c);
     }
+    // Grow the device's memory pool once, up front: the resident store and the
+    // workers' scratch are then carved from memory the pool already holds (its
+    // release threshold keeps freed memory), instead of growing it while
+    // requests wait.
+    {
+        void *p = nullptr;
+        const size_t warm = store_budget + (size_t)workers * (512ull << 20);
+        cudaStream_t st = s->ctxs[0]->stream;
+        cudaSetDevice(device);
+        if (cudaMallocAsync(&p, warm, st) == cudaSuccess) cudaFreeAsync(p, st);
+        cudaStreamSynchronize(st);
+        cudaGetLastError();
+    }
     for (uint32_t w = 0; w < workers; w++) s->threads.emplace_back(worker, s, w);
     *out = s;
     return OL_OK;
