@@ -58,12 +58,15 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-mb", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="enqueue the headline step call by call, no CUDA graph")
     ap.add_argument("--profile-launches", action="store_true",
                     help="one short run for an ncu launch list (no e2e, no CPU leg)")
     ap.add_argument("--workload", default="parse_search", choices=["parse_search", "dictionary", "batch", "serve"],
                     help="parse_search: 1 GiB parse + 8-pattern search (the headline); dictionary: 1 GiB x "
                          "10,000 patterns; batch: 10,000 uneven documents, batched vs one call per document; "
                          "serve: open-loop Poisson parse/search requests, concurrent workers vs one")
+    ap.add_argument("--pattern-source-bytes", type=int, default=0,
+                    help="sample the 8 patterns from the document of this size (the text is its prefix)")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the serve workload's arrival stream")
     ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean arrivals per second")
@@ -202,9 +205,15 @@ def barrier(world: int):
 
 # ------------------------------------------------------------------ workload
 
-def make_workload(nbytes: int, seed: int):
+def make_workload(nbytes: int, seed: int, pattern_source_bytes: int = 0):
+    """The document and its 8 patterns. With pattern_source_bytes > nbytes the
+    patterns are those of the larger document of the same seed, of which the text
+    is the prefix (profiling the full-size patterns on a smaller text)."""
     from oneline_b200 import datagen
 
+    if pattern_source_bytes > nbytes:
+        big = datagen.corpus(pattern_source_bytes, seed)
+        return np.ascontiguousarray(big[:nbytes]), datagen.patterns_eight(big, seed)
     text = datagen.corpus(nbytes, seed)
     pats = datagen.patterns_eight(text, seed)
     return text, pats
@@ -288,7 +297,7 @@ def run_ours(args, world, rank, local):
     from oneline_b200 import GpuParser, _lib
 
     L = _lib.load()
-    text, pats = make_workload(args.bytes, args.seed + rank)
+    text, pats = make_workload(args.bytes, args.seed + rank, args.pattern_source_bytes)
     N = text.size
     torch.cuda.set_device(local)
     p = GpuParser(local)
@@ -357,23 +366,34 @@ def run_ours(args, world, rank, local):
     t_tree = timed(enqueue_tree)
     t_search = timed(enqueue_search)
 
-    # Timed region.
+    # Timed region: the step replayed as one CUDA graph (or, with --no-graph,
+    # enqueued call by call).
+    run_step, tstream, per_step = step, stream, None
+    if not args.no_graph:
+        pipe = p.capture_pipeline(doc, tree, pats, maxes, d_tot.data_ptr(), [o.data_ptr() for o in outs])
+        run_step = pipe.launch
+        tstream = torch.cuda.ExternalStream(pipe.stream, device=f"cuda:{local}")
+        per_step = pipe.kernels
     for _ in range(args.warmup):
-        step()
+        run_step()
     p.sync()
+    torch.cuda.synchronize(local)
+    if not args.no_graph:
+        pipe.sync()
     barrier(world)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = L.ol_launch_count()
     with ClockSampler(local) as clocks:
-        with torch.cuda.stream(stream):
+        with torch.cuda.stream(tstream):
             ev0.record()
         for _ in range(args.steps):
-            step()
-        with torch.cuda.stream(stream):
+            run_step()
+        with torch.cuda.stream(tstream):
             ev1.record()
         ev1.synchronize()
-    launches = L.ol_launch_count() - l0
+    # graph replays launch the captured kernels without passing the library's counter
+    launches = per_step * args.steps if per_step is not None else L.ol_launch_count() - l0
     torch.cuda.synchronize()
     barrier(world)
     ms = ev0.elapsed_time(ev1) / args.steps
@@ -454,6 +474,7 @@ def run_ours(args, world, rank, local):
                 "config": {**workload_config(args, N, pats, lines), "hits": totals},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": int(launches), "clocks": clocks.summary(),
+                "step_form": "CUDA graph (ol_pipeline_launch)" if not args.no_graph else "enqueued calls",
                 "device": p.adapter_name()}
         print(json.dumps(line), flush=True)
 
@@ -487,6 +508,11 @@ def run_dictionary(args, world, rank, local):
         c, t = p.search_many_device(doc, ps, hits.data_ptr(), total)
         assert t == total
 
+    if args.profile_launches:
+        for _ in range(args.warmup + args.steps):
+            step()
+        p.sync()
+        return
     for _ in range(args.warmup):
         step()
     p.sync()
@@ -745,7 +771,7 @@ def serve_run(reqs, workers: int, warm_docs):
                         ready.append(r.doc_id)
                         sizes[r.doc_id] = nbytes
                 results.append((kind, r.status, r.latency_ns, nbytes if kind == "parse" else sizes.get(r.doc_id, 0),
-                                r.start_ns, r.end_ns))
+                                r.start_ns, r.end_ns, r.submit_ns))
                 i += 1
 
         col = threading.Thread(target=collect)
@@ -785,11 +811,18 @@ def run_serve(args, world, rank, local):
             res, wall, stats = serve_run(reqs, workers, warm)
         ok = [r for r in res if r[1] == 0]
         lat = np.array([r[2] for r in ok], np.float64) / 1e6
-        span = (max(r[5] for r in ok) - min(r[4] for r in ok)) / 1e9
+        wait = np.array([r[4] - r[6] for r in ok], np.float64) / 1e6  # queued before a worker took it
+        svc = np.array([r[5] - r[4] for r in ok], np.float64) / 1e6
+        by_kind = {k: np.array([r[2] for r in ok if r[0] == k], np.float64) / 1e6 for k in ("parse", "search")}
+        span = (max(r[5] for r in ok) - min(r[6] for r in ok)) / 1e9
         nbytes = sum(r[3] for r in ok)
         out[name] = {"workers": workers, "requests": len(res), "ok": len(ok),
                      "refused": sum(1 for r in res if r[1] == 6), "not_found": sum(1 for r in res if r[1] == 9),
                      "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                     "queue_p99_ms": round(float(np.percentile(wait, 99)), 3),
+                     "p99_ms_second_half": round(float(np.percentile(lat[len(lat) // 2:], 99)), 3),
+                     "service_p99_ms": round(float(np.percentile(svc, 99)), 3),
+                     "p99_ms_by_kind": {k: round(float(np.percentile(v, 99)), 3) for k, v in by_kind.items() if v.size},
                      "req_per_s": round(len(ok) / wall, 1), "gb_per_s": round(nbytes / span / 1e9, 3),
                      "wall_s": round(wall, 2), "store": stats, "clocks": clocks.summary()}
     sv, pl = out["served"], out["plain"]

@@ -174,6 +174,24 @@ ol_status ol_query_raw(ol_ctx *ctx, const uint8_t *text, uint64_t len, uint32_t 
 ol_status ol_query(ol_ctx *ctx, const uint8_t *text, uint64_t len, const uint32_t *offsets, uint64_t n_lines,
                    uint32_t kind, uint32_t depth, uint32_t max_matches, uint32_t *total, uint32_t *out);
 
+/* ---- the parse-then-search pipeline as one CUDA graph. No reference
+ *      counterpart. Captures, once, a re-parse of the resident document, its
+ *      tree links (into `tree`, already built for it) and a search of n
+ *      patterns (as ol_search_multi_async: d_totals, d_outs on the device);
+ *      ol_pipeline_launch then replays all of it with one graph launch on the
+ *      pipeline's own stream. The pipeline keeps private scratch memory; the
+ *      document, tree and output buffers must outlive it. */
+typedef struct ol_pipeline ol_pipeline;
+ol_status ol_pipeline_capture(ol_ctx *ctx, ol_doc *doc, ol_tree *tree, const uint8_t *const *patterns,
+                              const uint32_t *lens, uint32_t n, const uint32_t *max_matches, uint32_t *d_totals,
+                              uint32_t *const *d_outs, ol_pipeline **out);
+ol_status ol_pipeline_launch(ol_pipeline *pipeline);
+ol_status ol_pipeline_sync(ol_pipeline *pipeline);
+/* The stream replays run on (a cudaStream_t), and the kernels one replay launches. */
+void *ol_pipeline_stream(const ol_pipeline *pipeline);
+uint32_t ol_pipeline_kernels(const ol_pipeline *pipeline);
+void ol_pipeline_free(ol_pipeline *pipeline);
+
 /* ---- dictionary search: GpuParser::compile_patterns / search_many,
  *      GpuPatternSet::{len, is_empty} (crates/oneline-gpu/src/many.rs:139-176,
  *      391-399). A set holds 1..OL_MAX_DICT_PATTERNS patterns of

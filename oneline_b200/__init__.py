@@ -19,6 +19,7 @@ from .gpu import (  # noqa: F401
     GpuDocument,
     GpuParser,
     GpuPatternSet,
+    GpuPipeline,
     GpuTree,
     ManyResult,
     QueryResult,

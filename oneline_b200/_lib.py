@@ -65,6 +65,12 @@ SIGNATURES: dict[str, tuple] = {
     "ol_query_subtree": (_S, [_P, _P, _P, _U64, _U32, _U32, _U32, _U32P, _P]),
     "ol_query_raw": (_S, [_P, _U8P, _U64, _U32, _U32, _U32, _U32P, _P]),
     "ol_query": (_S, [_P, _U8P, _U64, _P, _U64, _U32, _U32, _U32, _U32P, _P]),
+    "ol_pipeline_capture": (_S, [_P, _P, _P, _P, _P, _U32, _P, _P, _P, _PP]),
+    "ol_pipeline_launch": (_S, [_P]),
+    "ol_pipeline_sync": (_S, [_P]),
+    "ol_pipeline_stream": (_P, [_P]),
+    "ol_pipeline_kernels": (_U32, [_P]),
+    "ol_pipeline_free": (None, [_P]),
     "ol_patset_compile": (_S, [_P, _P, _P, _P, _U32, _PP]),
     "ol_patset_free": (None, [_P]),
     "ol_patset_len": (_U32, [_P]),

@@ -91,6 +91,10 @@ uint32_t round_lines(uint64_t n);
 ol_status new_text_doc(ol_ctx *ctx, const uint8_t *text, uint64_t len, ol_doc **out);
 ol_status new_doc(ol_ctx *ctx, uint64_t len, ol_doc **out);
 ol_status parse_doc(ol_ctx *ctx, ol_doc *d, uint64_t est_lines, FlatNode **nodes_out);
+cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d);
+cudaError_t enqueue_tree(ol_ctx *ctx, const ol_doc *d, ol_tree *t);
+cudaError_t launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *dpats, const uint32_t *lens, uint32_t n,
+                         const uint32_t *max_out, uint32_t *d_totals, uint32_t *const *d_outs);
 ol_status many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits, uint32_t heavy_min_hits,
                    uint32_t *counts, uint64_t *total, ol_hit *host_hits, ol_hit *d_hits,
                    const unsigned long long *seg_start, const unsigned long long *seg_end, uint32_t n_seg);

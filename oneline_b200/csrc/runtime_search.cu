@@ -13,9 +13,9 @@
 
 using namespace ol;
 
-namespace {
+static uint32_t halo_for(uint32_t m) { return ((m > 0 ? m - 1 : 0) + 15u) & ~15u; }
 
-uint32_t halo_for(uint32_t m) { return ((m > 0 ? m - 1 : 0) + 15u) & ~15u; }
+namespace {
 
 // Enqueues searches of n patterns over doc, at most 8 per launch (longer than
 // the staged limit: one per launch). Results stay on the device: d_totals[i]
@@ -54,7 +54,24 @@ cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pa
     uint8_t *dpat = (uint8_t *)ctx->pattern_dev.ptr;
     if ((e = cudaMemcpyAsync(dpat, ctx->pat_host, std::max<size_t>(w, 1), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
     if ((e = cudaEventRecord(ctx->pat_done, st)) != cudaSuccess) return e;
+    std::vector<const uint8_t *> dp(n);
+    for (uint32_t i = 0; i < n; i++) dp[i] = dpat + at[i];
+    return ol::launch_multi(ctx, d, dp.data(), lens, n, max_out, d_totals, d_outs);
+}
 
+}  // namespace
+
+// Launches the searches of n patterns already in device memory (dpats[i]) over
+// doc, at most 8 per launch (longer than the staged limit: one per launch).
+// Only stream operations: a CUDA graph can capture it once the context's
+// scratch is large enough.
+cudaError_t ol::launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *dpats, const uint32_t *lens, uint32_t n,
+                             const uint32_t *max_out, uint32_t *d_totals, uint32_t *const *d_outs) {
+    cudaStream_t st = ctx->stream;
+    uint32_t n_tiles = (uint32_t)((d->text_len + kSearchTile - 1) / kSearchTile);
+    const size_t col_words = (size_t)scan_ld(n_tiles) * kSearchMaxPatterns;  // counts, then bases
+    cudaError_t e = ctx->scratch_a.reserve(col_words * 4 * 2, st);
+    if (e != cudaSuccess) return e;
     uint32_t i = 0;
     while (i < n) {
         SearchArgs a{};
@@ -63,14 +80,14 @@ cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pa
         a.n_tiles = n_tiles;
         a.ld = scan_ld(n_tiles);
         a.counts = (uint32_t *)ctx->scratch_a.ptr;
-        a.bases = (uint32_t *)ctx->scratch_a.ptr + (size_t)a.ld * kSearchMaxPatterns;
+        a.bases = (uint32_t *)ctx->scratch_a.ptr + col_words;
         uint32_t halo = 0;
         bool alone = halo_for(lens[i]) > kSearchMaxStagedPattern;
         uint32_t first = i;
         while (i < n && a.np < kSearchMaxPatterns) {
             bool long_pat = halo_for(lens[i]) > kSearchMaxStagedPattern;
             if (a.np > 0 && (alone || long_pat)) break;
-            a.pat[a.np] = dpat + at[i];
+            a.pat[a.np] = dpats[i];
             a.pat_len[a.np] = lens[i];
             a.out[a.np] = d_outs[i];
             a.max_out[a.np] = max_out[i];
@@ -85,6 +102,8 @@ cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pa
     }
     return cudaSuccess;
 }
+
+namespace {
 
 // Blocking multi-pattern search into host buffers.
 ol_status search_multi_host(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pats, const uint32_t *lens, uint32_t n,

@@ -117,6 +117,17 @@ ol_status build(ol_ctx *ctx, const ol_doc *d, ol_tree *t, uint32_t flags, bool w
 
 }  // namespace
 
+// The tree kernels for doc into t (sized for doc's lines), enqueued only: a
+// CUDA graph can capture it once t and the context's scratch are large enough.
+cudaError_t ol::enqueue_tree(ol_ctx *ctx, const ol_doc *d, ol_tree *t) {
+    const uint32_t L = d->line_count;
+    t->line_count = L;
+    if (L == 0) return cudaSuccess;
+    if (tree_alloc(ctx, t, L) != OL_OK) return cudaErrorMemoryAllocation;
+    t->deep = d->max_depth >= kTreeLevels;
+    return t->deep ? enqueue_tree_deep(ctx, d, t) : enqueue_tree_fast(ctx, d, t);
+}
+
 extern "C" ol_status ol_tree_build_reusing(ol_ctx *ctx, const ol_doc *d, ol_tree *previous, uint32_t flags, ol_tree **out) {
     if (!ctx || !d || !out) {
         if (previous) ol_tree_free(previous);

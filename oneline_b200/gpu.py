@@ -217,6 +217,42 @@ class GpuPatternSet:
             pass
 
 
+class GpuPipeline:
+    """A captured re-parse + tree + multi-pattern search of one resident document,
+    replayed as one CUDA graph launch (no reference counterpart)."""
+
+    def __init__(self, parser: "GpuParser", handle: int, keep):
+        self._parser = parser
+        self._h = handle
+        self._keep = keep
+        parser._children.add(self)
+
+    def launch(self) -> None:
+        check(_lib.load().ol_pipeline_launch(self._h))
+
+    def sync(self) -> None:
+        check(_lib.load().ol_pipeline_sync(self._h))
+
+    @property
+    def stream(self) -> int:
+        return int(_lib.load().ol_pipeline_stream(self._h) or 0)
+
+    @property
+    def kernels(self) -> int:
+        return int(_lib.load().ol_pipeline_kernels(self._h))
+
+    def free(self) -> None:
+        if self._h and self._parser._ctx:
+            _lib.load().ol_pipeline_free(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 class GpuBatch:
     """Many documents resident as one text (no reference counterpart: per document
     the results equal upload / build_tree / search_many on that document alone)."""
@@ -573,3 +609,23 @@ class GpuParser:
                                                int(heavy_min_hits), counts.ctypes.data, ctypes.byref(total),
                                                d_hits), self._ctx)
         return counts, int(total.value)
+
+    # ------------------------------------------------------------- pipeline
+
+    def capture_pipeline(self, doc: GpuDocument, tree: GpuTree, patterns, max_matches, d_totals: int,
+                         d_outs) -> GpuPipeline:
+        """Captures re-parse + tree + search of `patterns` over `doc` as one CUDA graph.
+        d_totals (u32 per pattern) and d_outs (one u32 buffer per pattern, room for
+        max_matches[i]) are device pointers that must outlive the pipeline."""
+        pats = [self._check_pattern(p, None) for p in patterns]
+        n = len(pats)
+        maxes = np.array([int(max_matches)] * n if np.isscalar(max_matches) else [int(m) for m in max_matches],
+                         np.uint32)
+        bufs = [np.frombuffer(p, np.uint8) for p in pats]
+        P = (ctypes.c_void_p * max(n, 1))(*[b.ctypes.data for b in bufs])
+        lens = np.array([len(p) for p in pats], np.uint32)
+        O = (ctypes.c_void_p * max(n, 1))(*[int(o) for o in d_outs])
+        h = ctypes.c_void_p()
+        check(_lib.load().ol_pipeline_capture(self._ctx, doc.handle, tree.handle, P, lens.ctypes.data, n,
+                                              maxes.ctypes.data, d_totals, O, ctypes.byref(h)), self._ctx)
+        return GpuPipeline(self, h.value, (doc, tree))
