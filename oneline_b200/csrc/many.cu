@@ -90,6 +90,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t pari
 // ------------------------------------------------------------ trie walk ----
 
 __device__ __forceinline__ uint32_t dict_child(const DictSet &s, const uint4 &nd, uint32_t b) {
+    if (nd.y & kDictDenseFlag) return __ldg(s.dense + (size_t)nd.w * 256 + b);
     const uint32_t n = nd.y;
     if (n == 0) return NONE;
     uint32_t e0 = nd.z & 0xFFu;

@@ -100,7 +100,14 @@ struct SearchArgs {
     uint32_t *counts;        // [np][ld] matches per tile (pass 1), 16-byte aligned
     uint32_t *bases;         // [np][ld] exclusive scans (pass 2), 16-byte aligned
     uint32_t *totals;        // kSearchMaxPatterns totals (pass 2)
+    // Staged form (nullptr: count pass + recomputing write pass): per tile a
+    // slot of stage_cap 16-bit tile offsets, and a flag per tile whose hits did
+    // not fit (recomputed by the write pass).
+    uint16_t *stage;
+    uint8_t *overflow;
+    uint32_t stage_cap;
 };
+constexpr uint32_t kSearchStageCap = 8192;  // staged hits per tile (all patterns of a launch)
 
 cudaError_t launch_search(const SearchArgs &a, cudaStream_t st);
 
@@ -151,10 +158,15 @@ struct DictSet {
     const uint2 *table;      // open addressing: {first 4 bytes, trie node at depth 4}; empty: .y == NONE
     uint32_t table_bits;
     uint32_t max_probe;      // longest probe distance of any key
-    const uint4 *nodes;      // {unique pattern ending here or NONE, edge count, edge 0, edge 1 | extra start}
-    const uint32_t *extra;   // edges 1.. of nodes with more than two; edge = (child << 8) | byte, sorted by byte
+    const uint4 *nodes;      // {unique pattern ending here or NONE, edge count (| kDictDenseFlag),
+                             //  edge 0, edge 1 | extra start | dense table}
+    const uint32_t *extra;   // edges 1.. of nodes with 3..kDictDenseMin children; edge = (child << 8) | byte,
+                             // sorted by byte
+    const uint32_t *dense;   // 256 children (NONE: no edge) per node with more than kDictDenseMin children
     uint32_t n_u;
 };
+constexpr uint32_t kDictDenseMin = 8;
+constexpr uint32_t kDictDenseFlag = 0x80000000u;
 
 struct DictMatchArgs {
     DictSet set;

@@ -135,6 +135,7 @@ extern "C" void ol_ctx_destroy(ol_ctx *ctx) {
     ctx->scratch_b.release(ctx->stream);
     ctx->scratch_c.release(ctx->stream);
     ctx->search_out.release(ctx->stream);
+    ctx->search_stage.release(ctx->stream);
     ctx->pattern_dev.release(ctx->stream);
     ctx->dict_small.release(ctx->stream);
     ctx->dict_bitmap.release(ctx->stream);

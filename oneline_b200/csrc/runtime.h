@@ -45,6 +45,7 @@ struct ol_ctx {
     ol::DevBuf scratch_b;  // second status array / uploaded offsets
     ol::DevBuf scratch_c;  // nodes and other per-call outputs
     ol::DevBuf search_out;
+    ol::DevBuf search_stage;  // staged search hits, 16 KiB per text tile
     ol::DevBuf pattern_dev;
     ol::DevBuf dict_small;   // dictionary search: per-pattern counts, ranks, slots
     ol::DevBuf dict_bitmap;  // heavy-pattern bitmaps

@@ -103,21 +103,30 @@ extern "C" ol_status ol_patset_compile(ol_ctx *ctx, const ol_doc *doc, const uin
     const uint32_t n_nodes = (uint32_t)trie.size();
     if (n_nodes >= (1u << 24)) return ctx_fail(ctx, OL_ERR_BAD_PATTERN, "pattern set too large for the trie");
     std::vector<uint4> nodes(n_nodes);
-    std::vector<uint32_t> extra;
+    std::vector<uint32_t> extra, dense;
     for (uint32_t v = 0; v < n_nodes; v++) {
         auto &k = trie[v].kids;
         std::sort(k.begin(), k.end());
         uint4 r{trie[v].out, (uint32_t)k.size(), 0, 0};
         auto pack = [](const std::pair<uint8_t, uint32_t> &e) { return (e.second << 8) | e.first; };
-        if (!k.empty()) r.z = pack(k[0]);
-        if (k.size() == 2) r.w = pack(k[1]);
-        if (k.size() > 2) {
-            r.w = (uint32_t)extra.size();
-            for (size_t i = 1; i < k.size(); i++) extra.push_back(pack(k[i]));
+        if (k.size() > kDictDenseMin) {
+            // many children: a 256-entry table, one load per step
+            r.y |= kDictDenseFlag;
+            r.w = (uint32_t)(dense.size() / 256);
+            dense.resize(dense.size() + 256, NONE);
+            for (auto &e : k) dense[(size_t)r.w * 256 + e.first] = e.second;
+        } else {
+            if (!k.empty()) r.z = pack(k[0]);
+            if (k.size() == 2) r.w = pack(k[1]);
+            if (k.size() > 2) {
+                r.w = (uint32_t)extra.size();
+                for (size_t i = 1; i < k.size(); i++) extra.push_back(pack(k[i]));
+            }
         }
         nodes[v] = r;
     }
     if (extra.empty()) extra.push_back(0);
+    if (dense.empty()) dense.push_back(NONE);
 
     // Filter and hash table over the distinct first-four-byte keys.
     std::vector<uint32_t> filter(1u << (kDictFilterBits - 5), 0);
@@ -153,7 +162,8 @@ extern "C" ol_status ol_patset_compile(ol_ctx *ctx, const ol_doc *doc, const uin
     size_t off_table = align256(off_filter + sz_filter), sz_table = table.size() * 8;
     size_t off_nodes = align256(off_table + sz_table), sz_nodes = nodes.size() * 16;
     size_t off_extra = align256(off_nodes + sz_nodes), sz_extra = extra.size() * 4;
-    size_t off_uid = align256(off_extra + sz_extra), sz_uid = (size_t)n * 4;
+    size_t off_dense = align256(off_extra + sz_extra), sz_dense = dense.size() * 4;
+    size_t off_uid = align256(off_dense + sz_dense), sz_uid = (size_t)n * 4;
     size_t off_ds = align256(off_uid + sz_uid), sz_ds = dup_start.size() * 4;
     size_t off_di = align256(off_ds + sz_ds), sz_di = dup_ids.size() * 4;
     size_t total = align256(off_di + sz_di);
@@ -162,6 +172,7 @@ extern "C" ol_status ol_patset_compile(ol_ctx *ctx, const ol_doc *doc, const uin
     memcpy(host.data() + off_table, table.data(), sz_table);
     memcpy(host.data() + off_nodes, nodes.data(), sz_nodes);
     memcpy(host.data() + off_extra, extra.data(), sz_extra);
+    memcpy(host.data() + off_dense, dense.data(), sz_dense);
     memcpy(host.data() + off_uid, u_of_id.data(), sz_uid);
     memcpy(host.data() + off_ds, dup_start.data(), sz_ds);
     memcpy(host.data() + off_di, dup_ids.data(), sz_di);
@@ -188,6 +199,7 @@ extern "C" ol_status ol_patset_compile(ol_ctx *ctx, const ol_doc *doc, const uin
     s->dev.max_probe = max_probe;
     s->dev.nodes = (const uint4 *)(b + off_nodes);
     s->dev.extra = (const uint32_t *)(b + off_extra);
+    s->dev.dense = (const uint32_t *)(b + off_dense);
     s->dev.n_u = U;
     s->u_of_id = (const uint32_t *)(b + off_uid);
     s->dup_start = (const uint32_t *)(b + off_ds);

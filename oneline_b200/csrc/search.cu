@@ -233,6 +233,7 @@ __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;
     const uint64_t t0 = (uint64_t)tile * kSearchTile;
+    if (a.stage && !a.overflow[tile]) return;  // written from the staged hits
     // patterns with matches here whose output window is not yet full
     uint32_t want = 0;
     for (uint32_t p = 0; p < a.np; p++) {
@@ -279,8 +280,121 @@ __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) 
     }
 }
 
+// ----------------------------------------------------------- staged path --
+//
+// With a staging buffer the filter and verification run once: pass 1
+// (search_stage_kernel) keeps each tile's match masks in shared memory, counts
+// every pattern's hits with one block scan for all patterns at once, and writes
+// the tile's hits, in (pattern, position) order, as 16-bit tile offsets into the
+// tile's staging slot. After the column scan, pass 2 (search_copy_kernel)
+// copies them to their final slots. A tile with more hits than its staging slot
+// holds is flagged and left to search_write_kernel, which recomputes it.
+
+__global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) {
+    __shared__ SearchSmem sm;
+    __shared__ uint16_t match[kSearchMaxPatterns][SR_PIECES];
+    __shared__ uint32_t warp_sum[SR_THREADS / 32][4];
+    __shared__ uint32_t tile_tot[kSearchMaxPatterns];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t tile = blockIdx.x;
+    const uint64_t t0 = (uint64_t)tile * kSearchTile;
+    uint4 v[SR_STEPS];
+    load_tile(a, sm, t0, v);
+    for (uint32_t o = tid; o < kSearchMaxPatterns * SR_PIECES / 8; o += SR_THREADS)
+        reinterpret_cast<uint4 *>(&match[0][0])[o] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    filter_tile(a, sm, v, (1u << a.np) - 1u, t0,
+                [&](uint32_t p, uint32_t piece, uint32_t mk) { match[p][piece] = (uint16_t)mk; });
+    __syncthreads();
+    // my hits per pattern (4 pieces: at most 64), two patterns per word
+    uint2 m4[kSearchMaxPatterns];
+    uint32_t packed[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (uint32_t p = 0; p < kSearchMaxPatterns; p++) {
+        m4[p] = p < a.np ? *reinterpret_cast<const uint2 *>(&match[p][4 * tid]) : make_uint2(0, 0);
+        packed[p >> 1] |= (uint32_t)(__popc(m4[p].x) + __popc(m4[p].y)) << (16 * (p & 1));
+    }
+    // inclusive warp scans of the packed counts (tile totals stay below 2^16)
+    uint32_t inc[4];
+#pragma unroll
+    for (uint32_t q = 0; q < 4; q++) {
+        inc[q] = packed[q];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc[q], o);
+            if ((int)lane >= o) inc[q] += t;
+        }
+        if (lane == 31) warp_sum[warp][q] = inc[q];
+    }
+    __syncthreads();
+    uint32_t before[4] = {0, 0, 0, 0}, total[4] = {0, 0, 0, 0};
+    for (uint32_t w = 0; w < SR_THREADS / 32; w++)
+#pragma unroll
+        for (uint32_t q = 0; q < 4; q++) {
+            before[q] += w < warp ? warp_sum[w][q] : 0u;
+            total[q] += warp_sum[w][q];
+        }
+    // tile totals per pattern, and where each pattern's hits start in the slot;
+    // the slot is assembled in shared memory (the staged text is no longer
+    // read) and stored with 16-byte writes
+    static_assert(kSearchStageCap * 2 <= kSearchTile, "the slot fits where the tile text was");
+    uint16_t *stage = reinterpret_cast<uint16_t *>(sm.text);
+    uint32_t start = 0;
+#pragma unroll
+    for (uint32_t p = 0; p < kSearchMaxPatterns; p++) {
+        const uint32_t sh = 16 * (p & 1);
+        const uint32_t tot = (total[p >> 1] >> sh) & 0xFFFFu;
+        const uint32_t mine = (packed[p >> 1] >> sh) & 0xFFFFu;
+        uint32_t r = start + ((before[p >> 1] >> sh) & 0xFFFFu) + ((inc[p >> 1] >> sh) & 0xFFFFu) - mine;
+        if (mine && start + tot <= a.stage_cap) {
+            const uint32_t mm[2] = {m4[p].x, m4[p].y};
+#pragma unroll
+            for (uint32_t h = 0; h < 2; h++) {
+                uint32_t bits = mm[h];
+                while (bits) {
+                    const uint32_t b = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    stage[r++] = (uint16_t)((4 * tid + 2 * h + (b >> 4)) * 16 + (b & 15));
+                }
+            }
+        }
+        if (tid == 0 && p < a.np) a.counts[(size_t)p * a.ld + tile] = tot;
+        start += tot;
+    }
+    if (tid == 0) a.overflow[tile] = start > a.stage_cap ? 1 : 0;
+    if (start == 0 || start > a.stage_cap) return;  // uniform: nothing to store, or recomputed later
+    __syncthreads();
+    uint4 *dst = reinterpret_cast<uint4 *>(a.stage + (size_t)tile * a.stage_cap);
+    const uint4 *src = reinterpret_cast<const uint4 *>(stage);
+    for (uint32_t o = tid; o < (start + 7) / 8; o += SR_THREADS) dst[o] = src[o];
+}
+
+__global__ void __launch_bounds__(SR_THREADS) search_copy_kernel(SearchArgs a) {
+    const uint32_t tile = blockIdx.x;
+    if (a.overflow[tile]) return;  // left to search_write_kernel
+    const uint64_t t0 = (uint64_t)tile * kSearchTile;
+    const uint16_t *slot = a.stage + (size_t)tile * a.stage_cap;
+    uint32_t start = 0;
+    for (uint32_t p = 0; p < a.np; p++) {
+        const size_t at = (size_t)p * a.ld + tile;
+        const uint32_t n = a.counts[at], base = a.bases[at], max_out = a.max_out[p];
+        uint32_t *out = a.out[p];
+        for (uint32_t i = threadIdx.x; i < n && base + i < max_out; i += SR_THREADS)
+            out[base + i] = (uint32_t)(t0 + slot[start + i]);
+        start += n;
+    }
+}
+
 cudaError_t launch_search(const SearchArgs &a, cudaStream_t st) {
     if (a.n_tiles == 0 || a.np == 0) return cudaSuccess;
+    if (a.stage) {
+        search_stage_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
+        cudaError_t e = launch_scan_columns(a.counts, a.bases, a.totals, a.n_tiles, a.np, a.ld, st);
+        if (e != cudaSuccess) return e;
+        search_copy_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
+        search_write_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();  // flagged tiles only
+        return cudaGetLastError();
+    }
     search_count_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
     cudaError_t e = launch_scan_columns(a.counts, a.bases, a.totals, a.n_tiles, a.np, a.ld, st);
     if (e != cudaSuccess) return e;
