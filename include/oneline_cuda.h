@@ -192,6 +192,31 @@ void *ol_pipeline_stream(const ol_pipeline *pipeline);
 uint32_t ol_pipeline_kernels(const ol_pipeline *pipeline);
 void ol_pipeline_free(ol_pipeline *pipeline);
 
+/* ---- tuning. No reference counterpart (the reference fixes its workgroup
+ *      sizes per shader). Kernel variants a context uses, chosen by measuring
+ *      them on a document with ol_autotune and recorded per device (name and SM
+ *      count) in a text file that ol_tuning_load reads back. The variants change
+ *      speed, never results. */
+typedef struct ol_tuning {
+    uint32_t dict_slice;          /* dictionary: text positions per warp work item (256, 512, 1024) */
+    uint32_t dict_blocks_per_sm;  /* dictionary: resident blocks per SM of the persistent pass (0: all that fit) */
+    uint32_t dict_heavy_divisor;  /* dictionary: patterns expected to occur text_len / divisor times or more
+                                     are collected as bitmaps */
+    uint32_t search_staged;       /* substring search: 1 stages each tile's hits in one pass, 0 counts then
+                                     recomputes in the writing pass */
+} ol_tuning;
+ol_status ol_tuning_get(ol_ctx *ctx, ol_tuning *out);
+ol_status ol_tuning_set(ol_ctx *ctx, const ol_tuning *tuning);
+/* Times the variants on doc: the dictionary variants with `set` (may be NULL),
+ * the search variants with the n patterns (n may be 0). Sets the fastest on
+ * ctx, writes them to *out, and records them in the file at `path` (may be
+ * NULL) under this device. */
+ol_status ol_autotune(ol_ctx *ctx, const ol_doc *doc, const ol_patset *set, const uint8_t *const *patterns,
+                      const uint32_t *lens, uint32_t n, const char *path, ol_tuning *out);
+/* Sets the variants recorded for this device in `path`; OL_ERR_NOT_FOUND when
+ * the file has none. */
+ol_status ol_tuning_load(ol_ctx *ctx, const char *path);
+
 /* ---- dictionary search: GpuParser::compile_patterns / search_many,
  *      GpuPatternSet::{len, is_empty} (crates/oneline-gpu/src/many.rs:139-176,
  *      391-399). A set holds 1..OL_MAX_DICT_PATTERNS patterns of

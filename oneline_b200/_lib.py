@@ -71,6 +71,10 @@ SIGNATURES: dict[str, tuple] = {
     "ol_pipeline_stream": (_P, [_P]),
     "ol_pipeline_kernels": (_U32, [_P]),
     "ol_pipeline_free": (None, [_P]),
+    "ol_tuning_get": (_S, [_P, _P]),
+    "ol_tuning_set": (_S, [_P, _P]),
+    "ol_autotune": (_S, [_P, _P, _P, _P, _P, _U32, ctypes.c_char_p, _P]),
+    "ol_tuning_load": (_S, [_P, ctypes.c_char_p]),
     "ol_patset_compile": (_S, [_P, _P, _P, _P, _U32, _PP]),
     "ol_patset_free": (None, [_P]),
     "ol_patset_len": (_U32, [_P]),

@@ -35,20 +35,19 @@ namespace ol {
 
 constexpr uint32_t DM_THREADS = 256;
 constexpr uint32_t DM_WARPS = DM_THREADS / 32;
-constexpr uint32_t DM_SLICE = 512;                        // text positions per warp work item
-constexpr uint32_t DM_SLICE_WORDS = DM_SLICE / 32;        // bitmap words per slice
-constexpr uint32_t DM_SLICES_PER_TILE = kDictTile / DM_SLICE;
-constexpr uint32_t DM_TEXT_BYTES = DM_SLICE + kDictHalo;  // staged per slice
 constexpr uint32_t DM_QCAP = 64;                          // per-warp candidate queue
 constexpr uint32_t DM_FILTER_WORDS = 1u << (kDictFilterBits - 5);
 constexpr uint32_t kMbarSpins = 1u << 24;
-static_assert(DM_TEXT_BYTES % 16 == 0, "16-byte staging");
-static_assert(kDictWordsPerTile % DM_SLICE_WORDS == 0, "slices tile the bitmap");
-
+// A warp's work item: SLICE text positions (staged with the longest pattern
+// after them) and their SLICE / 32 heavy-bitmap words per heavy pattern.
+template <uint32_t SLICE>
 struct DictSmem {
+    static constexpr uint32_t kWords = SLICE / 32;
+    static constexpr uint32_t kText = SLICE + kDictHalo;
+    static_assert(kText % 16 == 0 && kDictWordsPerTile % kWords == 0 && kDictTile % SLICE == 0, "slice geometry");
     uint32_t filter[DM_FILTER_WORDS];
-    alignas(16) uint8_t text[DM_WARPS][DM_TEXT_BYTES];
-    uint32_t stage[DM_WARPS][kDictMaxHeavy * DM_SLICE_WORDS];  // heavy bitmap words of the warp's slice
+    alignas(16) uint8_t text[DM_WARPS][kText];
+    uint32_t hmask[DM_WARPS][SLICE];  // per slice position: bit h = heavy pattern h starts there
     uint16_t queue[DM_WARPS][DM_QCAP];
     alignas(8) unsigned long long bar;
 };
@@ -120,8 +119,9 @@ __device__ __forceinline__ uint32_t dict_probe(const DictSet &s, uint32_t key) {
 
 // ------------------------------------------------------------- matching ----
 
-// Emits unique pattern u at absolute offset pos (slice-local position p).
-__device__ __forceinline__ void dict_emit(const DictMatchArgs &a, uint32_t *stage, uint32_t u, uint64_t pos, uint32_t p) {
+// Emits unique pattern u at absolute offset pos: counts (count mode), a bit of
+// the walk's heavy mask, or a light key.
+__device__ __forceinline__ void dict_emit(const DictMatchArgs &a, uint32_t &hm, uint32_t u, uint64_t pos) {
     if (a.count_only) {
         const uint32_t peers = __match_any_sync(__activemask(), u);
         if ((peers & ((1u << (threadIdx.x & 31)) - 1u)) == 0) atomicAdd(a.counts + u, (uint32_t)__popc(peers));
@@ -129,7 +129,7 @@ __device__ __forceinline__ void dict_emit(const DictMatchArgs &a, uint32_t *stag
     }
     const uint32_t hv = __ldg(a.heavy_of_u + u);
     if (hv != 0xFFu) {
-        atomicOr(stage + hv * DM_SLICE_WORDS + (p >> 5), 1u << (p & 31));
+        hm |= 1u << hv;
     } else {
         atomicAdd(a.counts + u, 1u);
         const uint32_t slot = atomicAdd(a.light_n, 1u);
@@ -140,19 +140,21 @@ __device__ __forceinline__ void dict_emit(const DictMatchArgs &a, uint32_t *stag
 // Every unique pattern starting at slice position p: probe the table with the
 // position's first four bytes, then walk the trie byte by byte. Hits must end
 // by `lim` (the end of the text, or of the position's document in a batch).
-__device__ __forceinline__ void dict_walk(const DictMatchArgs &a, const uint8_t *text, uint32_t *stage, uint32_t p,
-                                          uint64_t pos, uint64_t lim) {
+// Returns the heavy patterns found (bit h: heavy pattern h).
+__device__ __forceinline__ uint32_t dict_walk(const DictMatchArgs &a, const uint8_t *text, uint32_t p, uint64_t pos,
+                                              uint64_t lim) {
     const uint32_t key = (uint32_t)text[p] | ((uint32_t)text[p + 1] << 8) | ((uint32_t)text[p + 2] << 16) |
                          ((uint32_t)text[p + 3] << 24);
     uint32_t v = pos + kDictMinLen <= lim ? dict_probe(a.set, key) : NONE;
-    uint32_t d = kDictMinLen;
+    uint32_t d = kDictMinLen, hm = 0;
     while (v != NONE) {
         const uint4 nd = __ldg(a.set.nodes + v);
-        if (nd.x != NONE) dict_emit(a, stage, nd.x, pos, p);
+        if (nd.x != NONE) dict_emit(a, hm, nd.x, pos);
         if (d >= kDictMaxLen || pos + d >= lim) break;
         v = dict_child(a.set, nd, text[p + d]);
         d++;
     }
+    return hm;
 }
 
 // End of the document holding pos (pos itself when pos lies between
@@ -166,14 +168,20 @@ __device__ __forceinline__ uint64_t dict_limit(const DictMatchArgs &a, uint64_t 
     return a.seg_end[i];
 }
 
-// Each warp takes slices of 512 positions in turn: it stages the slice (plus
+// Each warp takes slices of SLICE positions in turn: it stages the slice (plus
 // the longest pattern) in its own shared memory, filters all positions 32 at a
 // time, queues the candidates and walks them 32 at a time (one per lane), so
-// walks run on full warps; heavy hits set bits in the slice's staged bitmap
-// words, written out once per slice. Warps never wait for one another.
+// walks run on full warps. A walk returns the heavy patterns of its position as
+// a 32-bit mask (no atomics); after the slice, ballots over each 32 positions'
+// masks transpose them into the heavy patterns' bitmap words, which lane h
+// stores for heavy pattern h. Warps never wait for one another.
+template <uint32_t SLICE>
 __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a) {
+    using Smem = DictSmem<SLICE>;
+    constexpr uint32_t DM_SLICE = SLICE, DM_SLICE_WORDS = Smem::kWords, DM_TEXT_BYTES = Smem::kText;
+    constexpr uint32_t DM_SLICES_PER_TILE = kDictTile / SLICE;
     extern __shared__ __align__(16) uint8_t dyn_smem[];
-    DictSmem &sm = *reinterpret_cast<DictSmem *>(dyn_smem);
+    Smem &sm = *reinterpret_cast<Smem *>(dyn_smem);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t lt = (1u << lane) - 1u;
 
@@ -196,7 +204,7 @@ __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a)
     const uint32_t n_items = ((a.n_tiles + a.tile_stride - 1) / a.tile_stride) * DM_SLICES_PER_TILE;
     const uint32_t H = a.count_only ? 0u : a.n_heavy;
     uint8_t *text = sm.text[warp];
-    uint32_t *stage = sm.stage[warp];
+    uint32_t *hmask = sm.hmask[warp];
     uint16_t *queue = sm.queue[warp];
 
     for (uint32_t item = blockIdx.x * DM_WARPS + warp; item < n_items; item += gridDim.x * DM_WARPS) {
@@ -205,7 +213,8 @@ __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a)
         __syncwarp();
         for (uint32_t o = lane * 16; o < DM_TEXT_BYTES; o += 32 * 16)
             *reinterpret_cast<uint4 *>(&text[o]) = ld_stream16(a.text + s0 + o);
-        for (uint32_t f = lane; f < H * DM_SLICE_WORDS; f += 32) stage[f] = 0;
+        if (H)
+            for (uint32_t f = lane; f < DM_SLICE; f += 32) hmask[f] = 0;
         __syncwarp();
         const uint32_t *tw = reinterpret_cast<const uint32_t *>(text);
         uint32_t hint = 0;
@@ -236,7 +245,8 @@ __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a)
             __syncwarp();
             if (qn >= 32) {  // walk 32 candidates, one per lane
                 const uint32_t q = queue[lane];
-                dict_walk(a, text, stage, q, s0 + q, dict_limit(a, s0 + q, hint));
+                const uint32_t hm = dict_walk(a, text, q, s0 + q, dict_limit(a, s0 + q, hint));
+                if (hm) hmask[q] = hm;
                 __syncwarp();
                 const uint16_t keep = lane + 32 < qn ? queue[lane + 32] : (uint16_t)0;
                 __syncwarp();
@@ -245,28 +255,64 @@ __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a)
                 __syncwarp();
             }
         }
-        if (lane < qn) dict_walk(a, text, stage, queue[lane], s0 + queue[lane], dict_limit(a, s0 + queue[lane], hint));
+        if (lane < qn) {
+            const uint32_t q = queue[lane];
+            const uint32_t hm = dict_walk(a, text, q, s0 + q, dict_limit(a, s0 + q, hint));
+            if (hm) hmask[q] = hm;
+        }
         __syncwarp();
-        // the slice's heavy bitmap words: 64 contiguous bytes per pattern
-        const uint32_t w0 = slice * DM_SLICE_WORDS;
-        for (uint32_t f = lane; f < H * DM_SLICE_WORDS; f += 32)
-            a.bitmap[(size_t)(f / DM_SLICE_WORDS) * n_words + w0 + (f % DM_SLICE_WORDS)] = stage[f];
+        if (H) {
+            // transpose: word w of heavy pattern h = ballot over positions 32w..32w+31 of bit h
+            uint32_t words[DM_SLICE_WORDS];
+#pragma unroll
+            for (uint32_t w = 0; w < DM_SLICE_WORDS; w++) {
+                const uint32_t m = hmask[w * 32 + lane];
+                uint32_t present = __reduce_or_sync(0xFFFFFFFFu, m);
+                words[w] = 0;
+                while (present) {
+                    const uint32_t h = __ffs(present) - 1;
+                    present &= present - 1;
+                    const uint32_t b = __ballot_sync(0xFFFFFFFFu, (m >> h) & 1u);
+                    if (lane == h) words[w] = b;
+                }
+            }
+            // lane h stores heavy pattern h's words of the slice (contiguous, 16-byte stores)
+            if (lane < H) {
+                uint4 *dst = reinterpret_cast<uint4 *>(a.bitmap + (size_t)lane * n_words + (size_t)slice * DM_SLICE_WORDS);
+#pragma unroll
+                for (uint32_t w = 0; w < DM_SLICE_WORDS; w += 4)
+                    dst[w / 4] = make_uint4(words[w], words[w + 1], words[w + 2], words[w + 3]);
+            }
+        }
     }
 }
 
-cudaError_t launch_dict_match(const DictMatchArgs &a, int sm_count, cudaStream_t st) {
-    if (a.n_tiles == 0) return cudaSuccess;
-    const size_t smem = sizeof(DictSmem);
-    cudaError_t e = cudaFuncSetAttribute(dict_match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+template <uint32_t SLICE>
+static cudaError_t launch_match(const DictMatchArgs &a, int sm_count, uint32_t blocks_per_sm, cudaStream_t st) {
+    const size_t smem = sizeof(DictSmem<SLICE>);
+    cudaError_t e = cudaFuncSetAttribute(dict_match_kernel<SLICE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dict_match_kernel, DM_THREADS, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dict_match_kernel<SLICE>, DM_THREADS, smem);
     if (e != cudaSuccess) return e;
-    const uint64_t n_items = (uint64_t)((a.n_tiles + a.tile_stride - 1) / a.tile_stride) * DM_SLICES_PER_TILE;
+    if (blocks_per_sm) per_sm = std::min<int>(per_sm, (int)blocks_per_sm);
+    const uint64_t n_items = (uint64_t)((a.n_tiles + a.tile_stride - 1) / a.tile_stride) * (kDictTile / SLICE);
     const uint32_t grid = (uint32_t)std::min<uint64_t>((n_items + DM_WARPS - 1) / DM_WARPS,
                                                        (uint64_t)std::max(per_sm, 1) * sm_count);
-    dict_match_kernel<<<grid, DM_THREADS, smem, st>>>(a); OL_LAUNCHED();
+    dict_match_kernel<SLICE><<<grid, DM_THREADS, smem, st>>>(a); OL_LAUNCHED();
     return cudaGetLastError();
+}
+
+// slice: text positions per warp work item (256, 512 or 1024); blocks_per_sm:
+// resident blocks per SM of the persistent grid (0: as many as fit).
+cudaError_t launch_dict_match(const DictMatchArgs &a, int sm_count, cudaStream_t st, uint32_t slice,
+                              uint32_t blocks_per_sm) {
+    if (a.n_tiles == 0) return cudaSuccess;
+    switch (slice) {
+        case 256: return launch_match<256>(a, sm_count, blocks_per_sm, st);
+        case 1024: return launch_match<1024>(a, sm_count, blocks_per_sm, st);
+        default: return launch_match<512>(a, sm_count, blocks_per_sm, st);
+    }
 }
 
 // ------------------------------------------------------------ heavy ranks --

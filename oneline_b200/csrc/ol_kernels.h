@@ -190,7 +190,8 @@ struct DictMatchArgs {
     uint32_t n_seg;
 };
 
-cudaError_t launch_dict_match(const DictMatchArgs &a, int sm_count, cudaStream_t st);
+cudaError_t launch_dict_match(const DictMatchArgs &a, int sm_count, cudaStream_t st, uint32_t slice = 512,
+                              uint32_t blocks_per_sm = 0);
 // Per (4096-word block, heavy pattern) popcounts, [n_heavy][ld] column-major.
 cudaError_t launch_dict_heavy_count(const uint32_t *bitmap, uint32_t n_words, uint32_t n_heavy, uint32_t *counts,
                                     uint32_t ld, cudaStream_t st);

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -123,6 +124,9 @@ extern "C" ol_status ol_ctx_create(int32_t device, ol_ctx **out) {
         ol_ctx_destroy(c);
         return OL_ERR_CUDA;
     }
+    // kernel variants recorded for this device by ol_autotune, when the
+    // environment names a tuning file (absent file or device: the defaults)
+    if (const char *tf = getenv("OL_TUNING_FILE")) load_tuning(c, tf);
     *out = c;
     return OL_OK;
 }

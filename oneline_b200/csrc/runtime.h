@@ -46,6 +46,7 @@ struct ol_ctx {
     ol::DevBuf scratch_c;  // nodes and other per-call outputs
     ol::DevBuf search_out;
     ol::DevBuf search_stage;  // staged search hits, 16 KiB per text tile
+    ol_tuning tune{512, 0, 512, 1};  // kernel variants in use (ol_autotune / ol_tuning_set)
     ol::DevBuf pattern_dev;
     ol::DevBuf dict_small;   // dictionary search: per-pattern counts, ranks, slots
     ol::DevBuf dict_bitmap;  // heavy-pattern bitmaps
@@ -96,6 +97,8 @@ cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d);
 cudaError_t enqueue_tree(ol_ctx *ctx, const ol_doc *d, ol_tree *t);
 cudaError_t launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *dpats, const uint32_t *lens, uint32_t n,
                          const uint32_t *max_out, uint32_t *d_totals, uint32_t *const *d_outs);
+// Sets ctx->tune from the line for ctx's device in the tuning file at path.
+ol_status load_tuning(ol_ctx *ctx, const char *path);
 ol_status many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits, uint32_t heavy_min_hits,
                    uint32_t *counts, uint64_t *total, ol_hit *host_hits, ol_hit *d_hits,
                    const unsigned long long *seg_start, const unsigned long long *seg_end, uint32_t n_seg);

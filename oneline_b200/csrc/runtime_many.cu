@@ -292,7 +292,7 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
     ma.n_seg = n_seg;
     e = cudaMemsetAsync(m.sample_counts, 0, (size_t)U * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(m.light_n, 0, 16, st);
-    if (e == cudaSuccess) e = launch_dict_match(ma, ctx->sm_count, st);
+    if (e == cudaSuccess) e = launch_dict_match(ma, ctx->sm_count, st, ctx->tune.dict_slice, ctx->tune.dict_blocks_per_sm);
     std::vector<uint32_t> sample(U);
     uint32_t flags[2] = {0, 0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(sample.data(), m.sample_counts, (size_t)U * 4, cudaMemcpyDeviceToHost, st);
@@ -301,7 +301,7 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "search_many sample");
     if (flags[1] & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "search_many: a bounded wait ran out");
     const double scale = (double)n_tiles / (double)n_work;
-    const double threshold = heavy_min_hits ? (double)heavy_min_hits : std::max(4096.0, (double)N / 512.0);
+    const double threshold = heavy_min_hits ? (double)heavy_min_hits : std::max(4096.0, (double)N / (double)std::max<uint32_t>(ctx->tune.dict_heavy_divisor, 1));
     std::vector<std::pair<double, uint32_t>> cand;
     double light_est = 0;
     for (uint32_t u = 0; u < U; u++) {
@@ -344,7 +344,7 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
         ma.light_keys = (unsigned long long *)ctx->dict_keys.ptr;
         ma.light_cap = (uint32_t)cap;
         ma.light_n = m.light_n;
-        if (e == cudaSuccess) e = launch_dict_match(ma, ctx->sm_count, st);
+        if (e == cudaSuccess) e = launch_dict_match(ma, ctx->sm_count, st, ctx->tune.dict_slice, ctx->tune.dict_blocks_per_sm);
         if (e == cudaSuccess) e = cudaMemcpyAsync(flags, m.light_n, 8, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "search_many match");

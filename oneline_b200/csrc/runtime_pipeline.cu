@@ -80,6 +80,7 @@ extern "C" ol_status ol_pipeline_capture(ol_ctx *ctx, ol_doc *d, ol_tree *t, con
         return ctx_fail(ctx, s, "pipeline: could not create its context");
     }
     ol_ctx *pc = p->pctx;
+    pc->tune = ctx->tune;
     // pattern copies, 16-byte aligned
     std::vector<size_t> at(n);
     size_t w = 0;

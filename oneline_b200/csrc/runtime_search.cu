@@ -73,7 +73,7 @@ cudaError_t ol::launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const 
     cudaError_t e = ctx->scratch_a.reserve(col_words * 4 * 2, st);
     // staging: kSearchStageCap tile offsets per tile, then the overflow flags
     const size_t stage_bytes = (size_t)n_tiles * kSearchStageCap * 2;
-    if (e == cudaSuccess) e = ctx->search_stage.reserve(stage_bytes + n_tiles + 16, st);
+    if (e == cudaSuccess && ctx->tune.search_staged) e = ctx->search_stage.reserve(stage_bytes + n_tiles + 16, st);
     if (e != cudaSuccess) return e;
     uint32_t i = 0;
     while (i < n) {
@@ -84,7 +84,7 @@ cudaError_t ol::launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const 
         a.ld = scan_ld(n_tiles);
         a.counts = (uint32_t *)ctx->scratch_a.ptr;
         a.bases = (uint32_t *)ctx->scratch_a.ptr + col_words;
-        a.stage = (uint16_t *)ctx->search_stage.ptr;
+        a.stage = ctx->tune.search_staged ? (uint16_t *)ctx->search_stage.ptr : nullptr;
         a.overflow = (uint8_t *)ctx->search_stage.ptr + stage_bytes;
         a.stage_cap = kSearchStageCap;
         uint32_t halo = 0;

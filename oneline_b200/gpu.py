@@ -160,6 +160,16 @@ class GpuTree:
             pass
 
 
+class Tuning(ctypes.Structure):
+    """ol_tuning: the kernel variants a context uses (speed only, never results)."""
+
+    _fields_ = [("dict_slice", ctypes.c_uint32), ("dict_blocks_per_sm", ctypes.c_uint32),
+                ("dict_heavy_divisor", ctypes.c_uint32), ("search_staged", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 @dataclass
 class QueryResult:
     """Result of a node query (query.rs:10-19): the number of matching lines and
@@ -629,3 +639,34 @@ class GpuParser:
         check(_lib.load().ol_pipeline_capture(self._ctx, doc.handle, tree.handle, P, lens.ctypes.data, n,
                                               maxes.ctypes.data, d_totals, O, ctypes.byref(h)), self._ctx)
         return GpuPipeline(self, h.value, (doc, tree))
+
+    # --------------------------------------------------------------- tuning
+
+    @property
+    def tuning(self) -> dict:
+        t = Tuning()
+        check(_lib.load().ol_tuning_get(self._ctx, ctypes.byref(t)), self._ctx)
+        return t.as_dict()
+
+    def set_tuning(self, **values) -> None:
+        t = Tuning(**{**self.tuning, **values})
+        check(_lib.load().ol_tuning_set(self._ctx, ctypes.byref(t)), self._ctx)
+
+    def autotune(self, doc: GpuDocument, pattern_set: "GpuPatternSet | None" = None, patterns=(),
+                 path: str | None = None) -> dict:
+        """Measures the kernel variants on `doc` (dictionary ones with `pattern_set`,
+        substring-search ones with `patterns`), keeps the fastest and records them
+        in the file at `path` under this device."""
+        pats = [self._check_pattern(p, None) for p in patterns]
+        bufs = [np.frombuffer(p, np.uint8) for p in pats]
+        P = (ctypes.c_void_p * max(len(pats), 1))(*[b.ctypes.data for b in bufs])
+        lens = np.array([len(p) for p in pats] or [0], np.uint32)
+        t = Tuning()
+        check(_lib.load().ol_autotune(self._ctx, doc.handle, pattern_set.handle if pattern_set else None, P,
+                                      lens.ctypes.data, len(pats), path.encode() if path else None, ctypes.byref(t)),
+              self._ctx)
+        return t.as_dict()
+
+    def tuning_load(self, path: str) -> dict:
+        check(_lib.load().ol_tuning_load(self._ctx, path.encode()), self._ctx)
+        return self.tuning
