@@ -537,6 +537,7 @@ def run_dictionary(args, world, rank, local):
             ev1.record()
         ev1.synchronize()
     launches = L.ol_launch_count() - l0
+    work = p.dict_stats()
     ms = allreduce_max(ev0.elapsed_time(ev1) / args.steps, world)
     bytes_all = allreduce_sum(float(N), world)
     value = bytes_all / (ms * 1e-3) / 1e9
@@ -595,6 +596,9 @@ def run_dictionary(args, world, rank, local):
                                        f"dictionary (4..64 B, 60% sampled from the text): every (pattern, offset)",
                            "text_bytes": int(N), "patterns": len(pats), "unique_patterns": ps.unique(),
                            "total_hits": int(total), "hit_bytes": int(8 * total),
+                           "walked_per_byte": round(work["walked"] / N, 4),
+                           "nodes_per_walk": round(work["nodes"] / max(work["walked"], 1), 2),
+                           "bitmap_patterns": work["heavy_patterns"], "sorted_key_hits": work["light_hits"],
                            "l2": "inputs and outputs larger than L2 (no flush needed)",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
                 "roofline": {"bound": "hbm", "kernel": "dictionary pass (match, rank, sort, emit)",

@@ -242,6 +242,11 @@ ol_status ol_search_many(ol_ctx *ctx, const ol_doc *doc, const ol_patset *set, u
  * keys (0: automatic). It changes the speed, never the result. */
 ol_status ol_search_many_device(ol_ctx *ctx, const ol_doc *doc, const ol_patset *set, uint64_t max_hits,
                                 uint32_t heavy_min_hits, uint32_t *counts, uint64_t *total_hits, ol_hit *d_hits);
+/* Work of the last dictionary search on ctx, for tuning and reports: out[0]
+ * text bytes, [1] positions walked in the trie (filter and table hits), [2] trie
+ * nodes visited, [3] patterns collected as bitmaps, [4] hits collected as sorted
+ * keys, [5] total hits. */
+ol_status ol_dict_stats(ol_ctx *ctx, uint64_t out[6]);
 
 /* ---- batches of documents. No counterpart in the reference, which handles
  *      one document per call (GpuParser::upload / build_tree / search_many,

@@ -75,6 +75,7 @@ SIGNATURES: dict[str, tuple] = {
     "ol_tuning_set": (_S, [_P, _P]),
     "ol_autotune": (_S, [_P, _P, _P, _P, _P, _U32, ctypes.c_char_p, _P]),
     "ol_tuning_load": (_S, [_P, ctypes.c_char_p]),
+    "ol_dict_stats": (_S, [_P, _P]),
     "ol_patset_compile": (_S, [_P, _P, _P, _P, _U32, _PP]),
     "ol_patset_free": (None, [_P]),
     "ol_patset_len": (_U32, [_P]),

@@ -142,13 +142,14 @@ __device__ __forceinline__ void dict_emit(const DictMatchArgs &a, uint32_t &hm, 
 // by `lim` (the end of the text, or of the position's document in a batch).
 // Returns the heavy patterns found (bit h: heavy pattern h).
 __device__ __forceinline__ uint32_t dict_walk(const DictMatchArgs &a, const uint8_t *text, uint32_t p, uint64_t pos,
-                                              uint64_t lim) {
+                                              uint64_t lim, uint32_t &levels) {
     const uint32_t key = (uint32_t)text[p] | ((uint32_t)text[p + 1] << 8) | ((uint32_t)text[p + 2] << 16) |
                          ((uint32_t)text[p + 3] << 24);
     uint32_t v = pos + kDictMinLen <= lim ? dict_probe(a.set, key) : NONE;
     uint32_t d = kDictMinLen, hm = 0;
     while (v != NONE) {
         const uint4 nd = __ldg(a.set.nodes + v);
+        levels++;
         if (nd.x != NONE) dict_emit(a, hm, nd.x, pos);
         if (d >= kDictMaxLen || pos + d >= lim) break;
         v = dict_child(a.set, nd, text[p + d]);
@@ -205,6 +206,7 @@ __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a)
     const uint32_t H = a.count_only ? 0u : a.n_heavy;
     uint8_t *text = sm.text[warp];
     uint32_t *hmask = sm.hmask[warp];
+    uint32_t cands = 0, levels = 0;  // per lane, for the search statistics
     uint16_t *queue = sm.queue[warp];
 
     for (uint32_t item = blockIdx.x * DM_WARPS + warp; item < n_items; item += gridDim.x * DM_WARPS) {
@@ -245,8 +247,9 @@ __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a)
             __syncwarp();
             if (qn >= 32) {  // walk 32 candidates, one per lane
                 const uint32_t q = queue[lane];
-                const uint32_t hm = dict_walk(a, text, q, s0 + q, dict_limit(a, s0 + q, hint));
+                const uint32_t hm = dict_walk(a, text, q, s0 + q, dict_limit(a, s0 + q, hint), levels);
                 if (hm) hmask[q] = hm;
+                cands++;
                 __syncwarp();
                 const uint16_t keep = lane + 32 < qn ? queue[lane + 32] : (uint16_t)0;
                 __syncwarp();
@@ -257,8 +260,9 @@ __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a)
         }
         if (lane < qn) {
             const uint32_t q = queue[lane];
-            const uint32_t hm = dict_walk(a, text, q, s0 + q, dict_limit(a, s0 + q, hint));
+            const uint32_t hm = dict_walk(a, text, q, s0 + q, dict_limit(a, s0 + q, hint), levels);
             if (hm) hmask[q] = hm;
+            cands++;
         }
         __syncwarp();
         if (H) {
@@ -283,6 +287,13 @@ __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a)
                 for (uint32_t w = 0; w < DM_SLICE_WORDS; w += 4)
                     dst[w / 4] = make_uint4(words[w], words[w + 1], words[w + 2], words[w + 3]);
             }
+        }
+    }
+    if (a.stats) {  // candidates walked and trie nodes visited
+        const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, cands), l = __reduce_add_sync(0xFFFFFFFFu, levels);
+        if (lane == 0) {
+            atomicAdd(a.stats, (unsigned long long)c);
+            atomicAdd(a.stats + 1, (unsigned long long)l);
         }
     }
 }

@@ -188,6 +188,7 @@ struct DictMatchArgs {
     const unsigned long long *seg_start;
     const unsigned long long *seg_end;
     uint32_t n_seg;
+    unsigned long long *stats;  // optional: += candidates walked, trie nodes visited
 };
 
 cudaError_t launch_dict_match(const DictMatchArgs &a, int sm_count, cudaStream_t st, uint32_t slice = 512,

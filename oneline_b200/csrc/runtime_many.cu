@@ -44,7 +44,7 @@ struct ManyScratch {
     uint32_t *sample_counts, *light_count, *light_base, *heavy_u, *heavy_totals, *heavy_counts, *heavy_bases;
     uint32_t *light_n, *error, *id_counts, *sort_hist, *sort_totals;
     uint8_t *heavy_of_u;
-    unsigned long long *id_base, *total;
+    unsigned long long *id_base, *total, *stats;
 };
 
 }  // namespace
@@ -249,7 +249,7 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
     size_t o_heavy_of = carve(at, U), o_heavy_u = carve(at, kDictMaxHeavy * 4), o_htot = carve(at, kDictMaxHeavy * 4);
     size_t o_hcounts = carve(at, (size_t)kDictMaxHeavy * hld * 4), o_hbases = carve(at, (size_t)kDictMaxHeavy * hld * 4);
     size_t o_ln = carve(at, 16), o_idc = carve(at, (size_t)n * 4), o_idb = carve(at, (size_t)n * 8), o_tot = carve(at, 16);
-    size_t o_stot = carve(at, 256 * 4);
+    size_t o_stot = carve(at, 256 * 4), o_stats = carve(at, 16);
     const size_t fixed = at;
     cudaError_t e = ctx->dict_small.reserve(fixed, st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "search_many");
@@ -269,6 +269,7 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
         m.id_base = (unsigned long long *)(b + o_idb);
         m.total = (unsigned long long *)(b + o_tot);
         m.sort_totals = (uint32_t *)(b + o_stot);
+        m.stats = (unsigned long long *)(b + o_stats);
         m.sort_hist = (uint32_t *)(b + fixed);
         return m;
     };
@@ -335,6 +336,8 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
         e = ctx->dict_keys.reserve((size_t)cap * 16, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(m.light_count, 0, (size_t)U * 4, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(m.light_n, 0, 16, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(m.stats, 0, 16, st);
+        ma.stats = m.stats;
         ma.tile_stride = 1;
         ma.count_only = 0;
         ma.counts = m.light_count;
@@ -405,9 +408,17 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
     unsigned long long tot = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&tot, m.total, 8, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(counts, m.id_counts, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
+    unsigned long long walk[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(walk, m.stats, 16, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "search_many ids");
     *total = tot;
+    ctx->dict_stats[0] = N;
+    ctx->dict_stats[1] = walk[0];
+    ctx->dict_stats[2] = walk[1];
+    ctx->dict_stats[3] = H;
+    ctx->dict_stats[4] = light_n;
+    ctx->dict_stats[5] = tot;
 
     // 4. Hits.
     const uint64_t k = std::min<uint64_t>(tot, max_hits);
@@ -443,4 +454,11 @@ extern "C" ol_status ol_search_many_device(ol_ctx *ctx, const ol_doc *d, const o
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
     return many_run(ctx, d, set, max_hits, heavy_min_hits, counts, total_hits, nullptr, d_hits, nullptr, nullptr, 0);
+}
+
+extern "C" ol_status ol_dict_stats(ol_ctx *ctx, uint64_t *out) {
+    if (!ctx || !out) return OL_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    for (int i = 0; i < 6; i++) out[i] = ctx->dict_stats[i];
+    return OL_OK;
 }

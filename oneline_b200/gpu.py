@@ -670,3 +670,11 @@ class GpuParser:
     def tuning_load(self, path: str) -> dict:
         check(_lib.load().ol_tuning_load(self._ctx, path.encode()), self._ctx)
         return self.tuning
+
+    def dict_stats(self) -> dict:
+        """Work of the last dictionary search: positions walked, trie nodes visited,
+        bitmap patterns, sorted-key hits, total hits."""
+        out = np.zeros(6, np.uint64)
+        check(_lib.load().ol_dict_stats(self._ctx, out.ctypes.data), self._ctx)
+        keys = ("text_bytes", "walked", "nodes", "heavy_patterns", "light_hits", "total_hits")
+        return {k: int(v) for k, v in zip(keys, out)}
