@@ -56,6 +56,7 @@ def parse_args():
     ap.add_argument("--bytes", type=int, default=1 << 30, help="document size (default 1 GiB)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-workers", type=int, default=2, help="concurrent end-to-end steps (contexts)")
     ap.add_argument("--cpu-sample-mb", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="enqueue the headline step call by call, no CUDA graph")
@@ -430,46 +431,59 @@ def run_ours(args, world, rank, local):
                 "ms_parse": round(t_parse, 4), "ms_tree": round(t_tree, 4),
                 "ms_search": round(t_search, 4)}
 
-    # End to end through the C ABI with host buffers.
+    # End to end through the C ABI with host buffers: `e2e_workers` host threads,
+    # each with its own context (stream) and pinned output buffers, run whole
+    # steps concurrently, so one step's upload overlaps another's downloads.
     e2e = None
     if args.e2e_steps > 0:
-        from oneline_b200 import NODE_DTYPE  # noqa: F401
+        import threading
 
-        offs_h = torch.empty(lines, dtype=torch.int32, pin_memory=True).numpy()
-        kinds_h = torch.empty(lines, dtype=torch.uint8, pin_memory=True).numpy()
-        tree_h = [torch.empty(lines, dtype=torch.int32, pin_memory=True).numpy() for _ in range(4)]
-        hits_h = [torch.empty(max(t, 1), dtype=torch.int32, pin_memory=True).numpy() for t in totals]
+        workers = max(1, args.e2e_workers)
+        ctxs = [p] + [GpuParser(local) for _ in range(workers - 1)]
 
-        tots_h = np.zeros(n_p, np.uint32)
-        OH = (ctypes.c_void_p * n_p)(*[a.ctypes.data for a in hits_h])
+        def make_step(q):
+            offs_h = torch.empty(lines, dtype=torch.int32, pin_memory=True).numpy()
+            kinds_h = torch.empty(lines, dtype=torch.uint8, pin_memory=True).numpy()
+            tree_h = [torch.empty(lines, dtype=torch.int32, pin_memory=True).numpy() for _ in range(4)]
+            hits_h = [torch.empty(max(t, 1), dtype=torch.int32, pin_memory=True).numpy() for t in totals]
+            tots_h = np.zeros(n_p, np.uint32)
+            OH = (ctypes.c_void_p * n_p)(*[a.ctypes.data for a in hits_h])
 
-        def e2e_step():
-            h = ctypes.c_void_p()
-            chk(L.ol_doc_upload(p.ctx, host.data_ptr(), N, ctypes.byref(h)))
-            t = ctypes.c_void_p()
-            chk(L.ol_tree_build(p.ctx, h.value, 1, ctypes.byref(t)))
-            chk(L.ol_search_multi(p.ctx, h.value, P, lens.ctypes.data, n_p, maxes.ctypes.data,
-                                  tots_h.ctypes.data, OH))
-            chk(L.ol_doc_read_offsets(p.ctx, h.value, offs_h.ctypes.data, lines))
-            chk(L.ol_doc_read_kinds(p.ctx, h.value, kinds_h.ctypes.data, lines))
-            chk(L.ol_tree_read(p.ctx, t.value, *[a.ctypes.data for a in tree_h], lines))
-            L.ol_tree_free(t.value)
-            L.ol_doc_free(h.value)
+            def e2e_step():
+                h = ctypes.c_void_p()
+                chk(L.ol_doc_upload(q.ctx, host.data_ptr(), N, ctypes.byref(h)))
+                t = ctypes.c_void_p()
+                chk(L.ol_tree_build(q.ctx, h.value, 1, ctypes.byref(t)))
+                chk(L.ol_search_multi(q.ctx, h.value, P, lens.ctypes.data, n_p, maxes.ctypes.data,
+                                      tots_h.ctypes.data, OH))
+                chk(L.ol_doc_read_offsets(q.ctx, h.value, offs_h.ctypes.data, lines))
+                chk(L.ol_doc_read_kinds(q.ctx, h.value, kinds_h.ctypes.data, lines))
+                chk(L.ol_tree_read(q.ctx, t.value, *[a.ctypes.data for a in tree_h], lines))
+                L.ol_tree_free(t.value)
+                L.ol_doc_free(h.value)
+                assert list(tots_h) == totals
+            return e2e_step
 
-        e2e_step()
-        p.sync()
+        steps = [make_step(q) for q in ctxs]
+        for f in steps:
+            f()  # warm-up: every context's buffers and kernels
         barrier(world)
+        threads = [threading.Thread(target=lambda f=f: [f() for _ in range(args.e2e_steps)]) for f in steps]
         t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            e2e_step()
-        p.sync()
-        dt = (time.perf_counter() - t0) / args.e2e_steps
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        dt = (time.perf_counter() - t0) / (args.e2e_steps * workers)
         dt = allreduce_max(dt, world)
+        for q in ctxs[1:]:
+            q.close()
         e2e = {"value": round(bytes_all / dt / 1e9, 4), "unit": "GB/s", "ms_per_step": round(dt * 1e3, 3),
                "h2d_bytes_per_step": int(N), "d2h_bytes_per_step": int(21 * lines + 4 * hits),
-               "timing": "host wall clock around blocking C-ABI calls, max over ranks",
-               "path": "ol_doc_upload (pinned) + ol_tree_build + ol_search_multi (8 patterns) + ol_doc_read_offsets/kinds + "
-                       "ol_tree_read (4 arrays)"}
+               "workers": workers,
+               "timing": "host wall clock around blocking C-ABI calls (steps of all workers / wall time), max over ranks",
+               "path": "per step: ol_doc_upload (pinned) + ol_tree_build + ol_search_multi (8 patterns) + "
+                       "ol_doc_read_offsets/kinds + ol_tree_read (4 arrays), on `workers` contexts at once"}
 
     cpu = None
     if rank == 0 and not args.no_cpu:
