@@ -120,12 +120,8 @@ extern "C" ol_status ol_search_noalloc(const uint8_t *d_text, uint64_t text_len,
     a.text = d_text;
     a.text_len = text_len;
     a.n_tiles = (uint32_t)((text_len + ol::kSearchTile - 1) / ol::kSearchTile);
-    a.np = 1;
     a.halo = (pat_len - 1 + 15u) & ~15u;
-    a.pat[0] = scratch;
-    a.pat_len[0] = pat_len;
-    a.out[0] = d_out;
-    a.max_out[0] = max_matches;
+    ol::search_add_pattern(a, pattern, scratch, pat_len, d_out, max_matches);
     a.ld = ol::scan_ld(a.n_tiles);
     a.counts = reinterpret_cast<uint32_t *>(scratch + kPatternBytes);
     a.bases = a.counts + kColumnWords;

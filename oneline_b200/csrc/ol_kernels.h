@@ -86,6 +86,16 @@ constexpr uint32_t kSearchTile = 16384;
 constexpr uint32_t kSearchMaxStagedPattern = 4096;
 constexpr uint32_t kSearchMaxPatterns = 8;  // patterns per launch
 
+// Per-pattern constants of a search launch, computed on the host from the
+// pattern bytes (search_add_pattern) and read by every block as kernel
+// parameters.
+struct SearchPatMeta {
+    uint32_t pre[4];  // bytes 0..3, each replicated into a word (0 past the end)
+    uint32_t anc[4];  // anchor words (len >= 7): bytes [r, r + 4) little-endian, r = 0..3
+    uint32_t len;
+    uint32_t f4;      // byte 0 replicated
+};
+
 struct SearchArgs {
     const uint8_t *text;     // padded: n_tiles * kSearchTile + kSearchMaxStagedPattern + 16 readable bytes
     uint64_t text_len;
@@ -106,9 +116,16 @@ struct SearchArgs {
     uint16_t *stage;
     uint8_t *overflow;
     uint32_t stage_cap;
+    SearchPatMeta meta[kSearchMaxPatterns];
+    uint32_t anchor_hash[kSearchMaxPatterns * 4];  // anchor-map bits of the patterns of >= 7 bytes
+    uint32_t n_anchor;
 };
 constexpr uint32_t kSearchStageCap = 8192;  // staged hits per tile (all patterns of a launch)
 
+// Appends a pattern to a launch (slot a.np): its device copy, and the
+// constants the kernels take from its host bytes.
+void search_add_pattern(SearchArgs &a, const uint8_t *host, const uint8_t *dev, uint32_t len, uint32_t *out,
+                        uint32_t max_out);
 cudaError_t launch_search(const SearchArgs &a, cudaStream_t st);
 
 // ---------------------------------------------------------------- query --

@@ -96,8 +96,9 @@ ol_status new_doc(ol_ctx *ctx, uint64_t len, ol_doc **out);
 ol_status parse_doc(ol_ctx *ctx, ol_doc *d, uint64_t est_lines, FlatNode **nodes_out);
 cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d);
 cudaError_t enqueue_tree(ol_ctx *ctx, const ol_doc *d, ol_tree *t);
-cudaError_t launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *dpats, const uint32_t *lens, uint32_t n,
-                         const uint32_t *max_out, uint32_t *d_totals, uint32_t *const *d_outs);
+cudaError_t launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *hpats, const uint8_t *const *dpats,
+                         const uint32_t *lens, uint32_t n, const uint32_t *max_out, uint32_t *d_totals,
+                         uint32_t *const *d_outs);
 // Sets ctx->tune from the line for ctx's device in the tuning file at path.
 ol_status load_tuning(ol_ctx *ctx, const char *path);
 ol_status many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits, uint32_t heavy_min_hits,

@@ -29,13 +29,13 @@ struct ol_pipeline {
 
 namespace {
 
-cudaError_t enqueue_step(ol_ctx *pctx, ol_doc *d, ol_tree *t, const std::vector<const uint8_t *> &dp,
-                         const std::vector<uint32_t> &lens, const uint32_t *max_matches, uint32_t *d_totals,
-                         uint32_t *const *d_outs) {
+cudaError_t enqueue_step(ol_ctx *pctx, ol_doc *d, ol_tree *t, const uint8_t *const *hp,
+                         const std::vector<const uint8_t *> &dp, const std::vector<uint32_t> &lens,
+                         const uint32_t *max_matches, uint32_t *d_totals, uint32_t *const *d_outs) {
     cudaError_t e = enqueue_parse(pctx, d);
     if (e == cudaSuccess) e = enqueue_tree(pctx, d, t);
     if (e == cudaSuccess && !dp.empty())
-        e = launch_multi(pctx, d, dp.data(), lens.data(), (uint32_t)dp.size(), max_matches, d_totals, d_outs);
+        e = launch_multi(pctx, d, hp, dp.data(), lens.data(), (uint32_t)dp.size(), max_matches, d_totals, d_outs);
     return e;
 }
 
@@ -97,14 +97,14 @@ extern "C" ol_status ol_pipeline_capture(ol_ctx *ctx, ol_doc *d, ol_tree *t, con
     for (uint32_t i = 0; i < n; i++) dp[i] = (const uint8_t *)p->patterns.ptr + at[i];
     // One plain run sizes every scratch buffer; the capture must then allocate nothing.
     const uint64_t l0 = ol_launch_count();
-    if (e == cudaSuccess) e = enqueue_step(pc, d, t, dp, ln, max_matches, d_totals, d_outs);
+    if (e == cudaSuccess) e = enqueue_step(pc, d, t, patterns, dp, ln, max_matches, d_totals, d_outs);
     if (e == cudaSuccess) e = cudaStreamSynchronize(pc->stream);
     p->kernels = (uint32_t)(ol_launch_count() - l0);
     void *before[6] = {pc->scratch_a.ptr, pc->scratch_b.ptr, pc->scratch_c.ptr, t->parent_buf.ptr, t->end_buf.ptr,
                        p->patterns.ptr};
     if (e == cudaSuccess) e = cudaStreamBeginCapture(pc->stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        cudaError_t ce = enqueue_step(pc, d, t, dp, ln, max_matches, d_totals, d_outs);
+        cudaError_t ce = enqueue_step(pc, d, t, patterns, dp, ln, max_matches, d_totals, d_outs);
         e = cudaStreamEndCapture(pc->stream, &p->graph);
         if (ce != cudaSuccess) e = ce;
     }

@@ -56,17 +56,18 @@ cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pa
     if ((e = cudaEventRecord(ctx->pat_done, st)) != cudaSuccess) return e;
     std::vector<const uint8_t *> dp(n);
     for (uint32_t i = 0; i < n; i++) dp[i] = dpat + at[i];
-    return ol::launch_multi(ctx, d, dp.data(), lens, n, max_out, d_totals, d_outs);
+    return ol::launch_multi(ctx, d, pats, dp.data(), lens, n, max_out, d_totals, d_outs);
 }
 
 }  // namespace
 
-// Launches the searches of n patterns already in device memory (dpats[i]) over
-// doc, at most 8 per launch (longer than the staged limit: one per launch).
-// Only stream operations: a CUDA graph can capture it once the context's
-// scratch is large enough.
-cudaError_t ol::launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *dpats, const uint32_t *lens, uint32_t n,
-                             const uint32_t *max_out, uint32_t *d_totals, uint32_t *const *d_outs) {
+// Launches the searches of n patterns already in device memory (dpats[i]; the
+// same bytes on the host: hpats[i]) over doc, at most 8 per launch (longer
+// than the staged limit: one per launch). Only stream operations: a CUDA
+// graph can capture it once the context's scratch is large enough.
+cudaError_t ol::launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *hpats, const uint8_t *const *dpats,
+                             const uint32_t *lens, uint32_t n, const uint32_t *max_out, uint32_t *d_totals,
+                             uint32_t *const *d_outs) {
     cudaStream_t st = ctx->stream;
     uint32_t n_tiles = (uint32_t)((d->text_len + kSearchTile - 1) / kSearchTile);
     const size_t col_words = (size_t)scan_ld(n_tiles) * kSearchMaxPatterns;  // counts, then bases
@@ -93,12 +94,8 @@ cudaError_t ol::launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const 
         while (i < n && a.np < kSearchMaxPatterns) {
             bool long_pat = halo_for(lens[i]) > kSearchMaxStagedPattern;
             if (a.np > 0 && (alone || long_pat)) break;
-            a.pat[a.np] = dpats[i];
-            a.pat_len[a.np] = lens[i];
-            a.out[a.np] = d_outs[i];
-            a.max_out[a.np] = max_out[i];
+            search_add_pattern(a, hpats[i], dpats[i], lens[i], d_outs[i], max_out[i]);
             halo = std::max(halo, halo_for(lens[i]));
-            a.np++;
             i++;
             if (alone) break;
         }

@@ -2,13 +2,17 @@
 //
 // Up to eight patterns are searched in one pass over the text; CTA b owns the
 // 16 KiB tile b and stages it, plus a halo of (longest pattern - 1) bytes, in
-// shared memory with 16-byte coalesced loads. For each pattern a first-byte
-// filter (byte SWAR over 16-byte pieces) queues candidate pieces per warp;
-// queued pieces are verified 32 at a time, one per lane: the last byte, then
-// every other byte, for all sixteen starts of the piece at once (byte SWAR on
-// shifted windows). An occurrence must end inside the text (the buffer is zero
-// padded: a pattern ending in NUL must not match the padding).
-// Three launches, no block waits on another:
+// shared memory with 16-byte coalesced loads. Every 16-byte piece is compared
+// with each pattern of up to 4 bytes at all sixteen starts at once (byte SWAR
+// on the piece shifted by 1, 2 and 3 bytes, built once for all patterns),
+// which decides it. Longer patterns only mark candidate pieces: 5-6 byte ones
+// by their first two bytes (the same SWAR), longer ones by a shared hash map
+// of their anchor words (the 4-byte-aligned text word inside every
+// occurrence). Candidate pieces are queued per warp and verified 32 at a
+// time, one per lane: the first byte, the last, then every other byte, all
+// sixteen starts at once. An occurrence must end inside the text (the buffer
+// is zero padded: a pattern ending in NUL must not match the padding).
+// Recomputing form, three launches, no block waits on another:
 //   1. search_count_kernel: matches per (tile, pattern);
 //   2. scan_columns_kernel: per pattern, the first output slot of every tile
 //      and the total;
@@ -36,18 +40,34 @@ constexpr uint32_t SR_PIECES = SR_THREADS * SR_STEPS;  // 16-byte pieces per til
 constexpr uint32_t SR_QCAP = 160;                       // per-warp candidate queue (< 32 left + 128 per pattern)
 static_assert(SR_THREADS * 16 * SR_STEPS == kSearchTile, "search tile");
 
-struct PatMeta {
+// Patterns of at least kAnchorMin bytes are filtered by their anchor words:
+// every occurrence at start s covers the 4-byte-aligned text word at
+// a = 4 * ceil(s / 4) (a - s <= 3), which equals the pattern's bytes
+// [a - s, a - s + 4) -- one of four anchor words. A 2^15-bit map of the
+// anchors' hashes, shared by all patterns of the launch, tells which aligned
+// text words may be one; those are compared exactly.
+constexpr uint32_t kAnchorMin = 7;
+constexpr uint32_t kAnchorBits = 15;
+
+__host__ __device__ __forceinline__ uint32_t anchor_hash(uint32_t w) {
+    return (w * 0x9E3779B1u) >> (32 - kAnchorBits);
+}
+
+struct alignas(16) PatMeta {
+    uint4 pre;  // bytes 0..3 of the pattern, each replicated into a word (unused ones 0)
+    uint4 anc;  // anchor words (len >= kAnchorMin)
     const uint8_t *ptr;
     uint32_t len;
     uint32_t f4;  // first byte, replicated
 };
 
 struct SearchSmem {
-    alignas(16) uint8_t text[kSearchTile + kSearchMaxStagedPattern + 16];  // write pass: output staging after use
+    alignas(16) uint8_t text[kSearchTile + kSearchMaxStagedPattern + 16];  // stage pass: output staging after use
+    uint32_t anchor_map[(1u << kAnchorBits) / 32];
     uint16_t queue[SR_THREADS / 32][SR_QCAP];  // (pattern << 10) | piece, per warp
     PatMeta pat[kSearchMaxPatterns];
     uint32_t count[kSearchMaxPatterns];
-    uint32_t active;  // write pass: patterns with matches in this tile (bit mask)
+    uint32_t active;  // stage pass: patterns with matches in this tile (bit mask)
 };
 
 // 16 bytes of shared memory starting at any byte offset.
@@ -83,6 +103,23 @@ __device__ __forceinline__ uint32_t gather16(uint32_t c0, uint32_t c1, uint32_t 
     return g(c0) | (g(c1) << 4) | (g(c2) << 8) | (g(c3) << 12);
 }
 
+// Clears the starts of the piece at tile-local lo that lie past N - m (they
+// cannot match; the zero padding must not complete a pattern ending in NUL).
+__device__ __forceinline__ void keep_valid_starts(uint64_t N, uint32_t m, uint64_t t0, uint32_t lo, uint32_t &c0,
+                                                  uint32_t &c1, uint32_t &c2, uint32_t &c3) {
+    const int64_t last_ok = (int64_t)N - (int64_t)m - (int64_t)t0;
+    uint32_t keep[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int64_t room = last_ok - (int64_t)(lo + 4 * i) + 1;  // valid starts in word i
+        keep[i] = room <= 0 ? 0u : (room >= 4 ? 0xFFFFFFFFu : ((1u << (8 * room)) - 1u));
+    }
+    c0 &= keep[0];
+    c1 &= keep[1];
+    c2 &= keep[2];
+    c3 &= keep[3];
+}
+
 // Exact matches of a pattern at the sixteen starts of one piece (piece x
 // covers tile bytes [16x, 16x+16)): first byte, then the last byte, then every
 // other byte, all sixteen starts at once.
@@ -93,19 +130,7 @@ __device__ __forceinline__ uint32_t verify_piece(const SearchArgs &a, const Sear
     const uint4 v = *reinterpret_cast<const uint4 *>(&sm.text[lo]);
     uint32_t c0 = zero_bytes(v.x ^ pm.f4), c1 = zero_bytes(v.y ^ pm.f4);
     uint32_t c2 = zero_bytes(v.z ^ pm.f4), c3 = zero_bytes(v.w ^ pm.f4);
-    if (tail_tile) {  // starts past N - m cannot match
-        const int64_t last_ok = (int64_t)a.text_len - (int64_t)m - (int64_t)t0;
-        uint32_t keep[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            int64_t room = last_ok - (int64_t)(lo + 4 * i) + 1;  // valid starts in word i
-            keep[i] = room <= 0 ? 0u : (room >= 4 ? 0xFFFFFFFFu : ((1u << (8 * room)) - 1u));
-        }
-        c0 &= keep[0];
-        c1 &= keep[1];
-        c2 &= keep[2];
-        c3 &= keep[3];
-    }
+    if (tail_tile) keep_valid_starts(a.text_len, m, t0, lo, c0, c1, c2, c3);
     for (uint32_t jj = 1; jj < m && (c0 | c1 | c2 | c3); jj++) {
         const uint32_t j = jj == 1 ? m - 1 : jj - 1;  // last byte first, then 1, 2, ...
         const uint32_t P4 = __ldg(pm.ptr + j) * 0x01010101u;
@@ -118,10 +143,13 @@ __device__ __forceinline__ uint32_t verify_piece(const SearchArgs &a, const Sear
     return gather16(c0, c1, c2, c3);
 }
 
-// Loads tile b (plus the halo) into shared memory and the pattern table.
-__device__ __forceinline__ void load_tile(const SearchArgs &a, SearchSmem &sm, uint64_t t0, uint4 v[SR_STEPS]) {
+// Loads tile b (plus the halo) into shared memory, and (warp 0) the pattern
+// table and the anchor map from the kernel parameters; the caller's
+// __syncthreads publishes them.
+__device__ __forceinline__ void load_tile(const SearchArgs &a, SearchSmem &sm, uint64_t t0) {
     const uint32_t tid = threadIdx.x;
     const bool staged = a.halo <= kSearchMaxStagedPattern;
+    uint4 v[SR_STEPS];
 #pragma unroll
     for (uint32_t k = 0; k < SR_STEPS; k++) v[k] = ld_stream16(a.text + t0 + k * 4096 + tid * 16);
 #pragma unroll
@@ -129,25 +157,51 @@ __device__ __forceinline__ void load_tile(const SearchArgs &a, SearchSmem &sm, u
     const uint32_t halo = staged ? a.halo : 0u;
     for (uint32_t o = tid * 16; o < halo; o += SR_THREADS * 16)
         *reinterpret_cast<uint4 *>(&sm.text[kSearchTile + o]) = ld_stream16(a.text + t0 + kSearchTile + o);
-    if (tid == 0) *reinterpret_cast<uint4 *>(&sm.text[kSearchTile + halo]) = make_uint4(0, 0, 0, 0);
-    if (tid < a.np) {
-        PatMeta pm;
-        pm.ptr = a.pat[tid];
-        pm.len = a.pat_len[tid];
-        pm.f4 = __ldg(pm.ptr) * 0x01010101u;
-        sm.pat[tid] = pm;
-        sm.count[tid] = 0;
+    // 16 bytes past the halo: zeros when staged; unstaged, the bytes right
+    // after the tile (the filter looks 3 bytes ahead; the text is padded)
+    if (tid == 0)
+        *reinterpret_cast<uint4 *>(&sm.text[kSearchTile + halo]) =
+            staged ? make_uint4(0, 0, 0, 0) : ld_stream16(a.text + t0 + kSearchTile);
+    if (tid < 32) {
+        uint4 *am = reinterpret_cast<uint4 *>(sm.anchor_map);
+        for (uint32_t o = tid; o < (1u << kAnchorBits) / 128; o += 32) am[o] = make_uint4(0, 0, 0, 0);
+        __syncwarp();
+        if (tid < a.n_anchor) {
+            const uint32_t h = a.anchor_hash[tid];
+            atomicOr(&sm.anchor_map[h >> 5], 1u << (h & 31));
+        }
+        if (tid < a.np) {
+            const SearchPatMeta &m = a.meta[tid];
+            PatMeta pm;
+            pm.ptr = a.pat[tid];
+            pm.len = m.len;
+            pm.f4 = m.f4;
+            pm.pre = make_uint4(m.pre[0], m.pre[1], m.pre[2], m.pre[3]);
+            pm.anc = make_uint4(m.anc[0], m.anc[1], m.anc[2], m.anc[3]);
+            sm.pat[tid] = pm;
+            sm.count[tid] = 0;
+        }
     }
 }
 
-// Runs the filter of every pattern in `mask` over the tile: every lane tests
-// its four pieces with the loose first-byte SWAR (three operations per word);
-// pieces with a candidate are queued per warp and verified 32 at a time, one
-// per lane, so verification work follows the number of candidates. `sink(p,
-// piece, matches)` receives every verified piece (matches may be 0).
-template <class Sink>
-__device__ __forceinline__ void filter_tile(const SearchArgs &a, SearchSmem &sm, const uint4 v[SR_STEPS], uint32_t mask,
-                                            uint64_t t0, Sink sink) {
+// Runs the filter of every pattern in `mask` over the tile (staged in shared
+// memory). Every lane takes its four pieces, one per step, and builds once for
+// all patterns the windows of the piece shifted by 1, 2 and 3 bytes (the word
+// after the piece comes from the next lane, or from shared memory for lane
+// 31). A pattern of at most 4 bytes is compared whole at all sixteen starts at
+// once (byte SWAR on the shifted windows) and its exact matches go to `sink`.
+// A pattern of 5 or 6 bytes marks the pieces where its first two bytes occur
+// (the same SWAR). Longer patterns share one test of the piece's five
+// anchoring aligned words against the anchor map, whose cost does not grow
+// with the number of patterns; a word found there is compared with each
+// pattern's anchors. Marked pieces are queued per warp and verified 32 at a
+// time, one per lane, so verification work follows the number of candidates.
+// Neither the step loop nor the pattern loops are unrolled: with up to eight
+// patterns an unrolled body outgrows the instruction cache. `sink(p, piece,
+// matches)` receives every verified piece (matches may be 0) and every
+// short-pattern piece with matches.
+template <uint32_t NP, class Sink>
+__device__ __forceinline__ void filter_tile(const SearchArgs &a, SearchSmem &sm, uint32_t mask, uint64_t t0, Sink sink) {
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool staged = a.halo <= kSearchMaxStagedPattern;
     const bool tail_tile = t0 + kSearchTile + a.halo + 16 > a.text_len;
@@ -162,17 +216,96 @@ __device__ __forceinline__ void filter_tile(const SearchArgs &a, SearchSmem &sm,
             }
         }
     };
-#pragma unroll 1
-    for (uint32_t p = 0; p < a.np; p++) {
-        if (!((mask >> p) & 1u)) continue;
-        const uint32_t F4 = sm.pat[p].f4;
-        uint32_t cm = 0;
+    uint32_t shorts = 0, mids = 0, anchored = 0;  // patterns in `mask` by length: <= 4, 5-6, >= 7
 #pragma unroll
-        for (uint32_t k = 0; k < SR_STEPS; k++) {
-            uint32_t c = zero_bytes_loose(v[k].x ^ F4) | zero_bytes_loose(v[k].y ^ F4) | zero_bytes_loose(v[k].z ^ F4) |
-                         zero_bytes_loose(v[k].w ^ F4);
-            cm |= (uint32_t)(c != 0) << k;
+    for (uint32_t p = 0; p < NP; p++) {
+        const uint32_t m = sm.pat[p].len;
+        if (!((mask >> p) & 1u)) continue;
+        if (m <= 4) shorts |= 1u << p;
+        else if (m < kAnchorMin) mids |= 1u << p;
+        else anchored |= 1u << p;
+    }
+    uint32_t cand = 0;  // bit 4p + k: piece k has a candidate of pattern p (patterns over 4 bytes)
+#pragma unroll 1
+    for (uint32_t k = 0; k < SR_STEPS; k++) {
+        const uint32_t piece = k * SR_THREADS + tid;
+        const uint4 vk = *reinterpret_cast<const uint4 *>(&sm.text[piece * 16]);
+        uint32_t w4 = __shfl_down_sync(0xFFFFFFFFu, vk.x, 1);
+        if (lane == 31) w4 = *reinterpret_cast<const uint32_t *>(&sm.text[(piece + 1) * 16]);
+        const uint32_t w[5] = {vk.x, vk.y, vk.z, vk.w, w4};
+        uint32_t s1[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) s1[i] = __funnelshift_r(w[i], w[i + 1], 8);
+        if (shorts) {  // uniform
+            uint32_t s2[4], s3[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                s2[i] = __funnelshift_r(w[i], w[i + 1], 16);
+                s3[i] = __funnelshift_r(w[i], w[i + 1], 24);
+            }
+#pragma unroll 1
+            for (uint32_t bits = shorts; bits; bits &= bits - 1) {
+                const uint32_t p = __ffs(bits) - 1;
+                const uint4 pre = sm.pat[p].pre;
+                const uint32_t m = sm.pat[p].len;
+                uint32_t x[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) x[i] = w[i] ^ pre.x;
+                if (m > 1)
+#pragma unroll
+                    for (int i = 0; i < 4; i++) x[i] |= s1[i] ^ pre.y;
+                if (m > 2)
+#pragma unroll
+                    for (int i = 0; i < 4; i++) x[i] |= s2[i] ^ pre.z;
+                if (m > 3)
+#pragma unroll
+                    for (int i = 0; i < 4; i++) x[i] |= s3[i] ^ pre.w;
+                uint32_t c0 = zero_bytes(x[0]), c1 = zero_bytes(x[1]), c2 = zero_bytes(x[2]), c3 = zero_bytes(x[3]);
+                if (tail_tile) keep_valid_starts(a.text_len, m, t0, piece * 16, c0, c1, c2, c3);
+                if (c0 | c1 | c2 | c3) sink(p, piece, gather16(c0, c1, c2, c3));
+            }
         }
+#pragma unroll 1
+        for (uint32_t bits = mids; bits; bits &= bits - 1) {  // the first two bytes (loose SWAR; exact as "any")
+            const uint32_t p = __ffs(bits) - 1;
+            const uint4 pre = sm.pat[p].pre;
+            uint32_t acc = 0;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t x = (w[i] ^ pre.x) | (s1[i] ^ pre.y);
+                acc |= (x - 0x01010101u) & ~x;
+            }
+            cand |= (uint32_t)((acc & 0x80808080u) != 0) << (4 * p + k);
+        }
+        if (anchored) {  // uniform
+            // the five aligned words that anchor the piece's sixteen starts:
+            // w[0] (start lo), w[1..3] (four starts each), w4 (lo+13..lo+15)
+            uint32_t hit = 0;
+#pragma unroll
+            for (int i = 0; i < 5; i++) {
+                const uint32_t h = anchor_hash(w[i]);
+                hit |= ((sm.anchor_map[h >> 5] >> (h & 31)) & 1u) << i;
+            }
+            if (hit) {  // rare: compare the anchors exactly
+#pragma unroll 1
+                for (uint32_t bits = anchored; bits; bits &= bits - 1) {
+                    const uint32_t p = __ffs(bits) - 1;
+                    const uint4 c = sm.pat[p].anc;
+                    bool any = (hit & 1u) && w[0] == c.x;
+#pragma unroll
+                    for (int i = 1; i < 4; i++)
+                        any |= ((hit >> i) & 1u) && (w[i] == c.x || w[i] == c.y || w[i] == c.z || w[i] == c.w);
+                    any |= ((hit >> 4) & 1u) && (w[4] == c.y || w[4] == c.z || w[4] == c.w);
+                    cand |= (uint32_t)any << (4 * p + k);
+                }
+            }
+        }
+    }
+#pragma unroll 1
+    for (uint32_t bits = mids | anchored; bits; bits &= bits - 1) {
+        const uint32_t p = __ffs(bits) - 1;
+        uint32_t cm = (cand >> (4 * p)) & 0xFu;
+        if (!__any_sync(0xFFFFFFFFu, cm != 0)) continue;
         uint32_t n = __popc(cm), inc = n;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -201,17 +334,17 @@ __device__ __forceinline__ void filter_tile(const SearchArgs &a, SearchSmem &sm,
     drain(qn);
 }
 
-// Pass 1: matches of every pattern in every tile (counts only).
+// Pass 1: matches of every pattern in every tile (counts only). NP = a.np.
+template <uint32_t NP>
 __global__ void __launch_bounds__(SR_THREADS) search_count_kernel(SearchArgs a) {
     __shared__ SearchSmem sm;
     const uint32_t tid = threadIdx.x;
     const uint64_t t0 = (uint64_t)blockIdx.x * kSearchTile;
-    uint4 v[SR_STEPS];
-    load_tile(a, sm, t0, v);
+    load_tile(a, sm, t0);
     __syncthreads();
     // Lanes verifying pieces of the same pattern add up their matches first:
     // one shared-memory atomic per (round, pattern) instead of one per piece.
-    filter_tile(a, sm, v, 0xFFu, t0, [&](uint32_t p, uint32_t piece, uint32_t mk) {
+    filter_tile<NP>(a, sm, 0xFFu, t0, [&](uint32_t p, uint32_t piece, uint32_t mk) {
         const uint32_t group = __match_any_sync(__activemask(), p);
         const uint32_t sum = __reduce_add_sync(group, __popc(mk));
         if ((threadIdx.x & 31) == __ffs(group) - 1 && sum) atomicAdd(&sm.count[p], sum);
@@ -226,9 +359,10 @@ __global__ void __launch_bounds__(SR_THREADS) search_count_kernel(SearchArgs a) 
 // thread its first output slot after the tile's base from pass 2, and each
 // thread writes its matches there: the block's stores cover one contiguous
 // range. Tiles without matches exit before loading text.
+template <uint32_t NP>
 __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) {
     __shared__ SearchSmem sm;
-    __shared__ uint16_t match[kSearchMaxPatterns][SR_PIECES];
+    __shared__ uint16_t match[NP][SR_PIECES];
     __shared__ uint32_t warp_sum[SR_THREADS / 32];
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;
@@ -236,17 +370,16 @@ __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) 
     if (a.stage && !a.overflow[tile]) return;  // written from the staged hits
     // patterns with matches here whose output window is not yet full
     uint32_t want = 0;
-    for (uint32_t p = 0; p < a.np; p++) {
+    for (uint32_t p = 0; p < NP; p++) {
         size_t at = (size_t)p * a.ld + tile;
         if (a.counts[at] && a.bases[at] < a.max_out[p]) want |= 1u << p;
     }
     if (!want) return;
-    uint4 v[SR_STEPS];
-    load_tile(a, sm, t0, v);
-    for (uint32_t o = tid; o < kSearchMaxPatterns * SR_PIECES / 8; o += SR_THREADS)
+    load_tile(a, sm, t0);
+    for (uint32_t o = tid; o < NP * SR_PIECES / 8; o += SR_THREADS)
         reinterpret_cast<uint4 *>(&match[0][0])[o] = make_uint4(0, 0, 0, 0);
     __syncthreads();
-    filter_tile(a, sm, v, want, t0, [&](uint32_t p, uint32_t piece, uint32_t mk) { match[p][piece] = (uint16_t)mk; });
+    filter_tile<NP>(a, sm, want, t0, [&](uint32_t p, uint32_t piece, uint32_t mk) { match[p][piece] = (uint16_t)mk; });
     __syncthreads();
     for (uint32_t w = want; w; w &= w - 1) {
         const uint32_t p = __ffs(w) - 1;
@@ -290,50 +423,73 @@ __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) 
 // copies them to their final slots. A tile with more hits than its staging slot
 // holds is flagged and left to search_write_kernel, which recomputes it.
 
+template <uint32_t NP>
 __global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) {
+    constexpr uint32_t NQ = (NP + 1) / 2;  // packed count words, two patterns each
     __shared__ SearchSmem sm;
-    __shared__ uint16_t match[kSearchMaxPatterns][SR_PIECES];
-    __shared__ uint32_t warp_sum[SR_THREADS / 32][4];
-    __shared__ uint32_t tile_tot[kSearchMaxPatterns];
+    __shared__ uint16_t match[NP][SR_PIECES];
+    __shared__ uint32_t warp_sum[SR_THREADS / 32][NQ];
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;
     const uint64_t t0 = (uint64_t)tile * kSearchTile;
-    uint4 v[SR_STEPS];
-    load_tile(a, sm, t0, v);
-    for (uint32_t o = tid; o < kSearchMaxPatterns * SR_PIECES / 8; o += SR_THREADS)
+    load_tile(a, sm, t0);
+    if (tid == 0) sm.active = 0;
+    for (uint32_t o = tid; o < NP * SR_PIECES / 8; o += SR_THREADS)
         reinterpret_cast<uint4 *>(&match[0][0])[o] = make_uint4(0, 0, 0, 0);
     __syncthreads();
-    filter_tile(a, sm, v, (1u << a.np) - 1u, t0,
-                [&](uint32_t p, uint32_t piece, uint32_t mk) { match[p][piece] = (uint16_t)mk; });
+    filter_tile<NP>(a, sm, (1u << NP) - 1u, t0,
+                    [&](uint32_t p, uint32_t piece, uint32_t mk) { match[p][piece] = (uint16_t)mk; });
     __syncthreads();
-    // my hits per pattern (4 pieces: at most 64), two patterns per word
-    uint2 m4[kSearchMaxPatterns];
-    uint32_t packed[4] = {0, 0, 0, 0};
+    // my hits per pattern (4 pieces: at most 64), and the patterns with hits
+    // anywhere in the tile: a tile without hits is done here
+    uint2 m4[NP];
+    uint32_t mine_any = 0;
 #pragma unroll
-    for (uint32_t p = 0; p < kSearchMaxPatterns; p++) {
-        m4[p] = p < a.np ? *reinterpret_cast<const uint2 *>(&match[p][4 * tid]) : make_uint2(0, 0);
-        packed[p >> 1] |= (uint32_t)(__popc(m4[p].x) + __popc(m4[p].y)) << (16 * (p & 1));
+    for (uint32_t p = 0; p < NP; p++) {
+        m4[p] = *reinterpret_cast<const uint2 *>(&match[p][4 * tid]);
+        mine_any |= (m4[p].x | m4[p].y) ? 1u << p : 0u;
     }
-    // inclusive warp scans of the packed counts (tile totals stay below 2^16)
-    uint32_t inc[4];
+    mine_any = __reduce_or_sync(0xFFFFFFFFu, mine_any);
+    if (lane == 0 && mine_any) atomicOr(&sm.active, mine_any);
+    __syncthreads();
+    const uint32_t active = sm.active;
+    if (active == 0) {
+        if (tid < NP) a.counts[(size_t)tid * a.ld + tile] = 0;
+        if (tid == 0) a.overflow[tile] = 0;
+        return;
+    }
+    // counts, two patterns per word; inclusive warp scans of the words that
+    // hold a pattern with hits (tile totals stay below 2^16)
+    uint32_t packed[NQ], inc[NQ];
 #pragma unroll
-    for (uint32_t q = 0; q < 4; q++) {
+    for (uint32_t q = 0; q < NQ; q++) packed[q] = 0;
+#pragma unroll
+    for (uint32_t p = 0; p < NP; p++)
+        packed[p >> 1] |= (uint32_t)(__popc(m4[p].x) + __popc(m4[p].y)) << (16 * (p & 1));
+#pragma unroll
+    for (uint32_t q = 0; q < NQ; q++) {
         inc[q] = packed[q];
+        if ((active >> (2 * q)) & 3u) {  // uniform
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc[q], o);
-            if ((int)lane >= o) inc[q] += t;
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc[q], o);
+                if ((int)lane >= o) inc[q] += t;
+            }
         }
         if (lane == 31) warp_sum[warp][q] = inc[q];
     }
     __syncthreads();
-    uint32_t before[4] = {0, 0, 0, 0}, total[4] = {0, 0, 0, 0};
-    for (uint32_t w = 0; w < SR_THREADS / 32; w++)
+    uint32_t before[NQ], total[NQ];
 #pragma unroll
-        for (uint32_t q = 0; q < 4; q++) {
-            before[q] += w < warp ? warp_sum[w][q] : 0u;
-            total[q] += warp_sum[w][q];
-        }
+    for (uint32_t q = 0; q < NQ; q++) {
+        before[q] = total[q] = 0;
+        if ((active >> (2 * q)) & 3u)
+            for (uint32_t w = 0; w < SR_THREADS / 32; w++) {
+                const uint32_t x = warp_sum[w][q];
+                before[q] += w < warp ? x : 0u;
+                total[q] += x;
+            }
+    }
     // tile totals per pattern, and where each pattern's hits start in the slot;
     // the slot is assembled in shared memory (the staged text is no longer
     // read) and stored with 16-byte writes
@@ -341,7 +497,7 @@ __global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) 
     uint16_t *stage = reinterpret_cast<uint16_t *>(sm.text);
     uint32_t start = 0;
 #pragma unroll
-    for (uint32_t p = 0; p < kSearchMaxPatterns; p++) {
+    for (uint32_t p = 0; p < NP; p++) {
         const uint32_t sh = 16 * (p & 1);
         const uint32_t tot = (total[p >> 1] >> sh) & 0xFFFFu;
         const uint32_t mine = (packed[p >> 1] >> sh) & 0xFFFFu;
@@ -358,48 +514,107 @@ __global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) 
                 }
             }
         }
-        if (tid == 0 && p < a.np) a.counts[(size_t)p * a.ld + tile] = tot;
+        if (tid == 0) a.counts[(size_t)p * a.ld + tile] = tot;
         start += tot;
     }
     if (tid == 0) a.overflow[tile] = start > a.stage_cap ? 1 : 0;
-    if (start == 0 || start > a.stage_cap) return;  // uniform: nothing to store, or recomputed later
+    if (start > a.stage_cap) return;  // uniform: recomputed later
     __syncthreads();
     uint4 *dst = reinterpret_cast<uint4 *>(a.stage + (size_t)tile * a.stage_cap);
     const uint4 *src = reinterpret_cast<const uint4 *>(stage);
     for (uint32_t o = tid; o < (start + 7) / 8; o += SR_THREADS) dst[o] = src[o];
 }
 
+// Pass 2 of the staged path: one warp per tile. Lane p reads pattern p's
+// count and first output slot (all patterns at once: one memory round trip),
+// a warp scan places each pattern's hits in the tile's slot, and the warp
+// copies them to their final slots, 32 per step.
+constexpr uint32_t SC_TILES = SR_THREADS / 32;  // tiles per block
 __global__ void __launch_bounds__(SR_THREADS) search_copy_kernel(SearchArgs a) {
-    const uint32_t tile = blockIdx.x;
-    if (a.overflow[tile]) return;  // left to search_write_kernel
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t tile = blockIdx.x * SC_TILES + (threadIdx.x >> 5);
+    if (tile >= a.n_tiles || a.overflow[tile]) return;  // overflowing tiles: search_write_kernel
+    uint32_t n = 0, base = 0, max_out = 0;
+    if (lane < a.np) {
+        const size_t at = (size_t)lane * a.ld + tile;
+        n = a.counts[at];
+        base = a.bases[at];
+        max_out = a.max_out[lane];
+    }
+    uint32_t inc = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if ((int)lane >= o) inc += t;
+    }
+    if (__shfl_sync(0xFFFFFFFFu, inc, 31) == 0) return;
     const uint64_t t0 = (uint64_t)tile * kSearchTile;
     const uint16_t *slot = a.stage + (size_t)tile * a.stage_cap;
-    uint32_t start = 0;
     for (uint32_t p = 0; p < a.np; p++) {
-        const size_t at = (size_t)p * a.ld + tile;
-        const uint32_t n = a.counts[at], base = a.bases[at], max_out = a.max_out[p];
-        uint32_t *out = a.out[p];
-        for (uint32_t i = threadIdx.x; i < n && base + i < max_out; i += SR_THREADS)
-            out[base + i] = (uint32_t)(t0 + slot[start + i]);
-        start += n;
+        const uint32_t np_ = __shfl_sync(0xFFFFFFFFu, n, p);
+        if (np_ == 0) continue;
+        const uint32_t b = __shfl_sync(0xFFFFFFFFu, base, p), mx = __shfl_sync(0xFFFFFFFFu, max_out, p);
+        const uint32_t start = __shfl_sync(0xFFFFFFFFu, inc - n, p);
+        const uint32_t lim = b >= mx ? 0u : min(np_, mx - b);  // the first max_out hits overall
+        uint32_t *out = a.out[p] + b;
+        const uint16_t *src = slot + start;
+#pragma unroll 4
+        for (uint32_t i = lane; i < lim; i += 32) out[i] = (uint32_t)(t0 + src[i]);
     }
 }
 
-cudaError_t launch_search(const SearchArgs &a, cudaStream_t st) {
-    if (a.n_tiles == 0 || a.np == 0) return cudaSuccess;
+void search_add_pattern(SearchArgs &a, const uint8_t *host, const uint8_t *dev, uint32_t len, uint32_t *out,
+                        uint32_t max_out) {
+    const uint32_t p = a.np++;
+    a.pat[p] = dev;
+    a.pat_len[p] = len;
+    a.out[p] = out;
+    a.max_out[p] = max_out;
+    SearchPatMeta &m = a.meta[p];
+    m = SearchPatMeta{};
+    m.len = len;
+    m.f4 = (len ? host[0] : 0u) * 0x01010101u;
+    for (uint32_t j = 0; j < 4 && j < len; j++) m.pre[j] = host[j] * 0x01010101u;
+    if (len >= kAnchorMin)
+        for (uint32_t r = 0; r < 4; r++) {
+            m.anc[r] = (uint32_t)host[r] | ((uint32_t)host[r + 1] << 8) | ((uint32_t)host[r + 2] << 16) |
+                       ((uint32_t)host[r + 3] << 24);
+            a.anchor_hash[a.n_anchor++] = anchor_hash(m.anc[r]);
+        }
+}
+
+template <uint32_t NP>
+static cudaError_t launch_search_np(const SearchArgs &a, cudaStream_t st) {
     if (a.stage) {
-        search_stage_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
+        search_stage_kernel<NP><<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
         cudaError_t e = launch_scan_columns(a.counts, a.bases, a.totals, a.n_tiles, a.np, a.ld, st);
         if (e != cudaSuccess) return e;
-        search_copy_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
-        search_write_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();  // flagged tiles only
+        search_copy_kernel<<<(a.n_tiles + SC_TILES - 1) / SC_TILES, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
+        search_write_kernel<NP><<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();  // flagged tiles only
         return cudaGetLastError();
     }
-    search_count_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
+    search_count_kernel<NP><<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
     cudaError_t e = launch_scan_columns(a.counts, a.bases, a.totals, a.n_tiles, a.np, a.ld, st);
     if (e != cudaSuccess) return e;
-    search_write_kernel<<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
+    search_write_kernel<NP><<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
     return cudaGetLastError();
+}
+
+// One instantiation per pattern count: the per-pattern loops unroll without
+// guards and the shared match arrays hold only the launch's patterns.
+cudaError_t launch_search(const SearchArgs &a, cudaStream_t st) {
+    if (a.n_tiles == 0 || a.np == 0) return cudaSuccess;
+    switch (a.np) {
+        case 1: return launch_search_np<1>(a, st);
+        case 2: return launch_search_np<2>(a, st);
+        case 3: return launch_search_np<3>(a, st);
+        case 4: return launch_search_np<4>(a, st);
+        case 5: return launch_search_np<5>(a, st);
+        case 6: return launch_search_np<6>(a, st);
+        case 7: return launch_search_np<7>(a, st);
+        case 8: return launch_search_np<8>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace ol
