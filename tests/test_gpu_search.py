@@ -135,3 +135,42 @@ def test_multi_pattern_passes_match_single_searches(parser):
     res = parser.search_document_multi(doc, pats[:8], 3)
     for w, r in zip(want[:8], res):
         assert r.total_matches == len(w) and np.array_equal(r.offsets, w[:3])
+
+
+def test_planted_occurrences_at_every_offset_around_tile_edges(parser):
+    """Occurrences of 5..33-byte patterns planted at every offset from 20
+    bytes before to 20 bytes after a 16 KiB tile edge, searched alone and in
+    eight-pattern passes that mix every filter (whole-pattern compare up to 4
+    bytes, two-byte filter for 5-6, anchor words from 7), including patterns
+    that share anchor words."""
+    rng = np.random.default_rng(41)
+    tile = 16384
+    for m in [5, 6, 7, 8, 9, 11, 12, 16, 33]:
+        base = rng.integers(33, 127, size=m, dtype=np.uint8).tobytes()
+        n_edges = 41
+        text = bytearray(rng.integers(33, 127, size=(n_edges + 1) * tile + 777, dtype=np.uint8).tobytes())
+        for t, d in enumerate(range(-20, 21), start=1):
+            at = t * tile + d
+            text[at: at + m] = base
+        text[len(text) - m:] = base  # one ending exactly at the end of the text
+        text = bytes(text)
+        pats = [base, base[1:] + b"~", base[:-1], base[2:], base[:4], base[:5], base[:6], base[:1]]
+        doc = parser.upload(text)
+        want = [oracle.find_all(text, p) for p in pats]
+        assert len(want[0]) == n_edges + 1
+        res = parser.search_document_multi(doc, pats, [max(len(w), 1) for w in want])
+        for p, w, r in zip(pats, want, res):
+            assert r.total_matches == len(w) and np.array_equal(r.offsets, w), (m, p)
+        for p, w in zip(pats[:4], want[:4]):
+            r = parser.search_document(doc, p, max(len(w), 1), max_pattern_len=None)
+            assert r.total_matches == len(w) and np.array_equal(r.offsets, w), (m, p)
+
+
+def test_patterns_ending_in_nul_do_not_match_the_padding(parser):
+    for text, pats in [(b"x" * 40_000 + b"abc", [b"abc\0", b"abc\0\0\0\0", b"bc\0\0\0\0\0\0\0", b"c\0"]),
+                       (b"y" * 16_381 + b"abcd\0", [b"abcd\0\0\0\0", b"d\0\0", b"abcd\0"])]:
+        doc = parser.upload(text)
+        want = [oracle.find_all(text, p) for p in pats]
+        res = parser.search_document_multi(doc, pats, 4)
+        for p, w, r in zip(pats, want, res):
+            assert r.total_matches == len(w) and np.array_equal(r.offsets, w), p
