@@ -97,10 +97,13 @@ __device__ __forceinline__ uint4 window16(const uint8_t *smem, uint32_t off, boo
     return *reinterpret_cast<uint4 *>(b);
 }
 
-// 16-bit mask (bit i = byte i) from the high bits of four SWAR words.
+// 16-bit mask (bit i = byte i) from the high bits of four SWAR words. One
+// multiply gathers two words: the high bits of c0 (moved to bits 0, 8, 16,
+// 24) and of c1 (bits 4, 12, 20, 28) land, shifted by 21, 14, 7 and 0, on bits
+// 21..28 in byte order; no two partial products meet, so nothing carries.
 __device__ __forceinline__ uint32_t gather16(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) {
-    auto g = [](uint32_t c) { return (((c >> 7) * 0x00204081u) >> 21) & 0xFu; };
-    return g(c0) | (g(c1) << 4) | (g(c2) << 8) | (g(c3) << 12);
+    auto g2 = [](uint32_t lo, uint32_t hi) { return ((((lo >> 7) | (hi >> 3)) * 0x00204081u) >> 21) & 0xFFu; };
+    return g2(c0, c1) | (g2(c2, c3) << 8);
 }
 
 // Clears the starts of the piece at tile-local lo that lie past N - m (they
@@ -556,10 +559,22 @@ __global__ void __launch_bounds__(SR_THREADS) search_copy_kernel(SearchArgs a) {
         const uint32_t b = __shfl_sync(0xFFFFFFFFu, base, p), mx = __shfl_sync(0xFFFFFFFFu, max_out, p);
         const uint32_t start = __shfl_sync(0xFFFFFFFFu, inc - n, p);
         const uint32_t lim = b >= mx ? 0u : min(np_, mx - b);  // the first max_out hits overall
-        uint32_t *out = a.out[p] + b;
-        const uint16_t *src = slot + start;
-#pragma unroll 4
-        for (uint32_t i = lane; i < lim; i += 32) out[i] = (uint32_t)(t0 + src[i]);
+        uint32_t *__restrict__ out = a.out[p] + b;
+        const uint16_t *__restrict__ src = slot + start;
+        // four independent loads in flight per lane before the stores
+        for (uint32_t i0 = 0; i0 < lim; i0 += 128) {
+            uint32_t v[4];
+#pragma unroll
+            for (uint32_t j = 0; j < 4; j++) {
+                const uint32_t i = i0 + j * 32 + lane;
+                v[j] = i < lim ? __ldg(src + i) : 0u;
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < 4; j++) {
+                const uint32_t i = i0 + j * 32 + lane;
+                if (i < lim) out[i] = (uint32_t)(t0 + v[j]);
+            }
+        }
     }
 }
 
