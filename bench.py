@@ -39,6 +39,19 @@ FALLBACK_HBM_GBS = 6650.0
 METRIC = "parse+search GB/s vs HBM peak"
 
 
+def profiled_traffic(name: str, key: str):
+    """DRAM bytes per launch recorded from an ncu capture in a profiles/
+    summary (a line `key: <bytes>`), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                if line.startswith(key + ":"):
+                    return int(line.split(":", 1)[1].strip())
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def hbm_peak():
     try:
         with open(PEAKS_FILE) as f:
@@ -420,13 +433,18 @@ def run_ours(args, world, rank, local):
     # algorithmic bytes: text read once per launch + every output byte once
     groups = {"parse pass (newline_count, scan, parse_tiles, fixup)": (t_parse, N + 6 * lines),
               "tree pass (summary, scan, resolve)": (t_tree, 2 * lines + 16 * lines),
-              "8-pattern search pass (search_count, scan, search_write)": (t_search, N + 4 * hits)}
+              "8-pattern search pass (search_stage, scan, search_copy, search_write)": (t_search, N + 4 * hits)}
     dom = max(groups, key=lambda k: groups[k][0])
     t_launch = groups[dom][0]
     alg = groups[dom][1]
     achieved = alg / (t_launch * 1e-3) / 1e9
+    traffic = None
+    if dom.startswith("8-pattern search") and N == 1 << 30 and args.seed == 1 and args.pattern_source_bytes in (0, N):
+        traffic = profiled_traffic("search_stage_copy_8patterns_256mib.md", "traffic_bytes_per_1gib_pass")
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": traffic,
+                "traffic_source": "ncu dram read+write of the pass's kernels at 256 MiB, x4 (profiles/)"
+                if traffic else None,
                 "alg_bytes_per_launch": int(alg), "ms_per_launch": round(t_launch, 4),
                 "ms_parse": round(t_parse, 4), "ms_tree": round(t_tree, 4),
                 "ms_search": round(t_search, 4)}
