@@ -571,11 +571,26 @@ __device__ __forceinline__ uint32_t select_bit(uint32_t w, uint32_t k) {
 // are written by the whole warp to consecutive slots: lane j of each 32 finds
 // its word by a binary search over the round's word prefix sums and its bit by
 // select, so every store instruction covers 32 consecutive hits.
+// The ids of a unique pattern and their first output slots are read once per
+// block into shared memory (up to DH_MAX_DUPS of them), not once per 32 hits.
+constexpr uint32_t DH_MAX_DUPS = 64;
+
 __global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArgs a) {
     __shared__ uint32_t warp_tot[DH_THREADS / 32];
+    __shared__ uint32_t dup_id[DH_MAX_DUPS];
+    __shared__ unsigned long long dup_base[DH_MAX_DUPS];
     const uint32_t h = blockIdx.y, b = blockIdx.x;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t *col = a.bitmap + (size_t)h * a.n_words;
+    const uint32_t u = a.heavy_u[h];
+    const uint32_t d0 = a.dup_start[u], d1 = a.dup_start[u + 1];
+    const uint32_t n_dup = d1 - d0;
+    const bool cached = n_dup <= DH_MAX_DUPS;
+    if (cached && threadIdx.x < n_dup) {
+        const uint32_t id = __ldg(a.dup_ids + d0 + threadIdx.x);
+        dup_id[threadIdx.x] = id;
+        dup_base[threadIdx.x] = a.id_base[id];
+    }
     const uint32_t w0 = b * DH_WORDS + warp * (DH_WORDS / (DH_THREADS / 32));
     constexpr uint32_t kRounds = DH_WORDS / (DH_THREADS / 32) / 32;  // 16
     uint32_t c = 0;
@@ -590,10 +605,6 @@ __global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArg
     uint32_t rank = a.heavy_bases[(size_t)h * a.ld + b];
     for (uint32_t w = 0; w < warp; w++) rank += warp_tot[w];
     if (c == 0) return;  // uniform over the warp
-    const uint32_t u = a.heavy_u[h];
-    const uint32_t d0 = a.dup_start[u], d1 = a.dup_start[u + 1];
-    const uint32_t lt = (1u << lane) - 1u;
-    (void)lt;
     for (uint32_t r = 0; r < kRounds; r++) {
         const uint32_t idx = w0 + r * 32 + lane;
         const uint32_t word = idx < a.n_words ? __ldg(col + idx) : 0u;
@@ -619,10 +630,17 @@ __global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArg
             const uint32_t ei = __shfl_sync(0xFFFFFFFFu, excl, i);
             if (j < T) {
                 const uint32_t off = (w0 + r * 32 + i) * 32 + select_bit(wi, j - ei);
-                for (uint32_t d = d0; d < d1; d++) {
-                    const uint32_t id = __ldg(a.dup_ids + d);
-                    const unsigned long long slot = a.id_base[id] + rank + j;
-                    if (slot < a.max_hits) a.hits[slot] = make_uint2(id, off);
+                if (cached) {
+                    for (uint32_t d = 0; d < n_dup; d++) {
+                        const unsigned long long slot = dup_base[d] + rank + j;
+                        if (slot < a.max_hits) __stcs(&a.hits[slot], make_uint2(dup_id[d], off));  // streamed: never re-read here
+                    }
+                } else {
+                    for (uint32_t d = d0; d < d1; d++) {
+                        const uint32_t id = __ldg(a.dup_ids + d);
+                        const unsigned long long slot = a.id_base[id] + rank + j;
+                        if (slot < a.max_hits) a.hits[slot] = make_uint2(id, off);
+                    }
                 }
             }
         }

@@ -5,7 +5,7 @@
 // shared memory with 16-byte coalesced loads. Every 16-byte piece is compared
 // with each pattern of up to 4 bytes at all sixteen starts at once (byte SWAR
 // on the piece shifted by 1, 2 and 3 bytes, built once for all patterns),
-// which decides it. Longer patterns only mark candidate pieces: 5-6 byte ones
+// which decides it. Longer patterns only mark candidate pieces: 5-7 byte ones
 // by their first two bytes (the same SWAR), longer ones by a shared hash map
 // of their anchor words (the 4-byte-aligned text word inside every
 // occurrence). Candidate pieces are queued per warp and verified 32 at a
@@ -42,11 +42,13 @@ static_assert(SR_THREADS * 16 * SR_STEPS == kSearchTile, "search tile");
 
 // Patterns of at least kAnchorMin bytes are filtered by their anchor words:
 // every occurrence at start s covers the 4-byte-aligned text word at
-// a = 4 * ceil(s / 4) (a - s <= 3), which equals the pattern's bytes
-// [a - s, a - s + 4) -- one of four anchor words. A 2^15-bit map of the
-// anchors' hashes, shared by all patterns of the launch, tells which aligned
-// text words may be one; those are compared exactly.
-constexpr uint32_t kAnchorMin = 7;
+// a = 4 * floor(s / 4) + 4 (1 <= a - s <= 4, and a + 4 <= s + 8 <= s + len),
+// which equals the pattern's bytes [a - s, a - s + 4) -- one of four anchor
+// words, r = a - s = 1..4. The starts of the 16-byte piece at lo map to the
+// words at lo + 4, lo + 8, lo + 12 and lo + 16, four phases each. A 2^15-bit
+// map of the anchors' hashes, shared by all patterns of the launch, tells
+// which aligned text words may be one; those are compared exactly.
+constexpr uint32_t kAnchorMin = 8;
 constexpr uint32_t kAnchorBits = 15;
 
 __host__ __device__ __forceinline__ uint32_t anchor_hash(uint32_t w) {
@@ -55,7 +57,7 @@ __host__ __device__ __forceinline__ uint32_t anchor_hash(uint32_t w) {
 
 struct alignas(16) PatMeta {
     uint4 pre;  // bytes 0..3 of the pattern, each replicated into a word (unused ones 0)
-    uint4 anc;  // anchor words (len >= kAnchorMin)
+    uint4 anc;  // anchor words r = 1..4 (len >= kAnchorMin)
     const uint8_t *ptr;
     uint32_t len;
     uint32_t f4;  // first byte, replicated
@@ -193,8 +195,8 @@ __device__ __forceinline__ void load_tile(const SearchArgs &a, SearchSmem &sm, u
 // after the piece comes from the next lane, or from shared memory for lane
 // 31). A pattern of at most 4 bytes is compared whole at all sixteen starts at
 // once (byte SWAR on the shifted windows) and its exact matches go to `sink`.
-// A pattern of 5 or 6 bytes marks the pieces where its first two bytes occur
-// (the same SWAR). Longer patterns share one test of the piece's five
+// A pattern of 5 to 7 bytes marks the pieces where its first two bytes occur
+// (the same SWAR). Longer patterns share one test of the piece's four
 // anchoring aligned words against the anchor map, whose cost does not grow
 // with the number of patterns; a word found there is compared with each
 // pattern's anchors. Marked pieces are queued per warp and verified 32 at a
@@ -219,7 +221,7 @@ __device__ __forceinline__ void filter_tile(const SearchArgs &a, SearchSmem &sm,
             }
         }
     };
-    uint32_t shorts = 0, mids = 0, anchored = 0;  // patterns in `mask` by length: <= 4, 5-6, >= 7
+    uint32_t shorts = 0, mids = 0, anchored = 0;  // patterns in `mask` by length: <= 4, 5-7, >= 8
 #pragma unroll
     for (uint32_t p = 0; p < NP; p++) {
         const uint32_t m = sm.pat[p].len;
@@ -281,24 +283,22 @@ __device__ __forceinline__ void filter_tile(const SearchArgs &a, SearchSmem &sm,
             cand |= (uint32_t)((acc & 0x80808080u) != 0) << (4 * p + k);
         }
         if (anchored) {  // uniform
-            // the five aligned words that anchor the piece's sixteen starts:
-            // w[0] (start lo), w[1..3] (four starts each), w4 (lo+13..lo+15)
+            // the four aligned words that anchor the piece's sixteen starts:
+            // w[i] anchors the starts lo + 4i - 4 .. lo + 4i - 1 (i = 1..4)
             uint32_t hit = 0;
 #pragma unroll
-            for (int i = 0; i < 5; i++) {
+            for (int i = 1; i < 5; i++) {
                 const uint32_t h = anchor_hash(w[i]);
-                hit |= ((sm.anchor_map[h >> 5] >> (h & 31)) & 1u) << i;
+                hit |= (sm.anchor_map[h >> 5] >> (h & 31)) & 1u;
             }
             if (hit) {  // rare: compare the anchors exactly
 #pragma unroll 1
                 for (uint32_t bits = anchored; bits; bits &= bits - 1) {
                     const uint32_t p = __ffs(bits) - 1;
                     const uint4 c = sm.pat[p].anc;
-                    bool any = (hit & 1u) && w[0] == c.x;
+                    bool any = false;
 #pragma unroll
-                    for (int i = 1; i < 4; i++)
-                        any |= ((hit >> i) & 1u) && (w[i] == c.x || w[i] == c.y || w[i] == c.z || w[i] == c.w);
-                    any |= ((hit >> 4) & 1u) && (w[4] == c.y || w[4] == c.z || w[4] == c.w);
+                    for (int i = 1; i < 5; i++) any |= w[i] == c.x || w[i] == c.y || w[i] == c.z || w[i] == c.w;
                     cand |= (uint32_t)any << (4 * p + k);
                 }
             }
@@ -591,10 +591,10 @@ void search_add_pattern(SearchArgs &a, const uint8_t *host, const uint8_t *dev, 
     m.f4 = (len ? host[0] : 0u) * 0x01010101u;
     for (uint32_t j = 0; j < 4 && j < len; j++) m.pre[j] = host[j] * 0x01010101u;
     if (len >= kAnchorMin)
-        for (uint32_t r = 0; r < 4; r++) {
-            m.anc[r] = (uint32_t)host[r] | ((uint32_t)host[r + 1] << 8) | ((uint32_t)host[r + 2] << 16) |
-                       ((uint32_t)host[r + 3] << 24);
-            a.anchor_hash[a.n_anchor++] = anchor_hash(m.anc[r]);
+        for (uint32_t r = 1; r <= 4; r++) {  // len >= 8: bytes r..r+3 exist
+            m.anc[r - 1] = (uint32_t)host[r] | ((uint32_t)host[r + 1] << 8) | ((uint32_t)host[r + 2] << 16) |
+                           ((uint32_t)host[r + 3] << 24);
+            a.anchor_hash[a.n_anchor++] = anchor_hash(m.anc[r - 1]);
         }
 }
 

@@ -141,7 +141,7 @@ def test_planted_occurrences_at_every_offset_around_tile_edges(parser):
     """Occurrences of 5..33-byte patterns planted at every offset from 20
     bytes before to 20 bytes after a 16 KiB tile edge, searched alone and in
     eight-pattern passes that mix every filter (whole-pattern compare up to 4
-    bytes, two-byte filter for 5-6, anchor words from 7), including patterns
+    bytes, two-byte filter for 5-7, anchor words from 8), including patterns
     that share anchor words."""
     rng = np.random.default_rng(41)
     tile = 16384
