@@ -224,6 +224,15 @@ __device__ __forceinline__ uint32_t eq_mask16(uint4 v, uint32_t c4) {
     return eq_mask4(v.x, c4) | (eq_mask4(v.y, c4) << 4) | (eq_mask4(v.z, c4) << 8) | (eq_mask4(v.w, c4) << 12);
 }
 
+// 16-bit mask (bit i = byte i) from the high bits of four SWAR words. One
+// multiply gathers two words: the high bits of c0 (moved to bits 0, 8, 16,
+// 24) and of c1 (bits 4, 12, 20, 28) land, shifted by 21, 14, 7 and 0, on bits
+// 21..28 in byte order; no two partial products meet, so nothing carries.
+__device__ __forceinline__ uint32_t gather16(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) {
+    auto g2 = [](uint32_t lo, uint32_t hi) { return ((((lo >> 7) | (hi >> 3)) * 0x00204081u) >> 21) & 0xFFu; };
+    return g2(c0, c1) | (g2(c2, c3) << 8);
+}
+
 __device__ __forceinline__ bool is_blank(uint8_t b) { return b == ' ' || b == '\t'; }
 
 // classify_line (crates/oneline-simd/src/line.rs:57-81) on the first content

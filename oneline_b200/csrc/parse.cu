@@ -237,15 +237,14 @@ __global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a)
             uint32_t rr = (k & 1) ? ((k < 2 ? r01 : r23) >> 16) : ((k < 2 ? r01 : r23) & 0xFFFF);
             int32_t rk = (int32_t)(sm.warp_base[k][warp] + rr) - w0;
             if (rk > (int32_t)PT_LIST) continue;
-#pragma unroll
-            for (uint32_t i = 0; i < 4; i++) {
-                uint32_t zz = z[k][i];
-                while (zz) {
-                    uint32_t b = (__ffs(zz) - 8) >> 3;
-                    zz &= zz - 1;
-                    if (rk >= 0 && rk <= (int32_t)PT_LIST) sm.nl[rk] = (uint16_t)(k * 4096 + tid * 16 + 4 * i + b);
-                    rk++;
-                }
+            // one loop over the piece's 16-bit newline mask: the warp runs as
+            // many rounds as its busiest lane has newlines in this piece
+            uint32_t m = gather16(z[k][0], z[k][1], z[k][2], z[k][3]);
+            while (m) {
+                const uint32_t b = __ffs(m) - 1;
+                m &= m - 1;
+                if (rk >= 0 && rk <= (int32_t)PT_LIST) sm.nl[rk] = (uint16_t)(k * 4096 + tid * 16 + b);
+                rk++;
             }
         }
         __syncthreads();  // (c) list ready

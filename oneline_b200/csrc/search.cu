@@ -99,15 +99,6 @@ __device__ __forceinline__ uint4 window16(const uint8_t *smem, uint32_t off, boo
     return *reinterpret_cast<uint4 *>(b);
 }
 
-// 16-bit mask (bit i = byte i) from the high bits of four SWAR words. One
-// multiply gathers two words: the high bits of c0 (moved to bits 0, 8, 16,
-// 24) and of c1 (bits 4, 12, 20, 28) land, shifted by 21, 14, 7 and 0, on bits
-// 21..28 in byte order; no two partial products meet, so nothing carries.
-__device__ __forceinline__ uint32_t gather16(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) {
-    auto g2 = [](uint32_t lo, uint32_t hi) { return ((((lo >> 7) | (hi >> 3)) * 0x00204081u) >> 21) & 0xFFu; };
-    return g2(c0, c1) | (g2(c2, c3) << 8);
-}
-
 // Clears the starts of the piece at tile-local lo that lie past N - m (they
 // cannot match; the zero padding must not complete a pattern ending in NUL).
 __device__ __forceinline__ void keep_valid_starts(uint64_t N, uint32_t m, uint64_t t0, uint32_t lo, uint32_t &c0,
