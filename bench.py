@@ -69,7 +69,7 @@ def parse_args():
     ap.add_argument("--bytes", type=int, default=1 << 30, help="document size (default 1 GiB)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--e2e-workers", type=int, default=2, help="concurrent end-to-end steps (contexts)")
+    ap.add_argument("--e2e-workers", type=int, default=3, help="concurrent end-to-end steps (contexts)")
     ap.add_argument("--cpu-sample-mb", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="enqueue the headline step call by call, no CUDA graph")
@@ -451,13 +451,17 @@ def run_ours(args, world, rank, local):
 
     # End to end through the C ABI with host buffers: `e2e_workers` host threads,
     # each with its own context (stream) and pinned output buffers, run whole
-    # steps concurrently, so one step's upload overlaps another's downloads.
+    # steps concurrently. One lock per copy direction keeps one upload and one
+    # download in flight at a time: each gets the link to itself, and one
+    # step's upload overlaps another's downloads instead of the threads
+    # uploading (then downloading) at the same time.
     e2e = None
     if args.e2e_steps > 0:
         import threading
 
         workers = max(1, args.e2e_workers)
         ctxs = [p] + [GpuParser(local) for _ in range(workers - 1)]
+        h2d_lock, d2h_lock = threading.Lock(), threading.Lock()
 
         def make_step(q):
             offs_h = torch.empty(lines, dtype=torch.int32, pin_memory=True).numpy()
@@ -469,14 +473,16 @@ def run_ours(args, world, rank, local):
 
             def e2e_step():
                 h = ctypes.c_void_p()
-                chk(L.ol_doc_upload(q.ctx, host.data_ptr(), N, ctypes.byref(h)))
+                with h2d_lock:
+                    chk(L.ol_doc_upload(q.ctx, host.data_ptr(), N, ctypes.byref(h)))
                 t = ctypes.c_void_p()
                 chk(L.ol_tree_build(q.ctx, h.value, 1, ctypes.byref(t)))
-                chk(L.ol_search_multi(q.ctx, h.value, P, lens.ctypes.data, n_p, maxes.ctypes.data,
-                                      tots_h.ctypes.data, OH))
-                chk(L.ol_doc_read_offsets(q.ctx, h.value, offs_h.ctypes.data, lines))
-                chk(L.ol_doc_read_kinds(q.ctx, h.value, kinds_h.ctypes.data, lines))
-                chk(L.ol_tree_read(q.ctx, t.value, *[a.ctypes.data for a in tree_h], lines))
+                with d2h_lock:
+                    chk(L.ol_search_multi(q.ctx, h.value, P, lens.ctypes.data, n_p, maxes.ctypes.data,
+                                          tots_h.ctypes.data, OH))
+                    chk(L.ol_doc_read_offsets(q.ctx, h.value, offs_h.ctypes.data, lines))
+                    chk(L.ol_doc_read_kinds(q.ctx, h.value, kinds_h.ctypes.data, lines))
+                    chk(L.ol_tree_read(q.ctx, t.value, *[a.ctypes.data for a in tree_h], lines))
                 L.ol_tree_free(t.value)
                 L.ol_doc_free(h.value)
                 assert list(tots_h) == totals
@@ -501,7 +507,8 @@ def run_ours(args, world, rank, local):
                "workers": workers,
                "timing": "host wall clock around blocking C-ABI calls (steps of all workers / wall time), max over ranks",
                "path": "per step: ol_doc_upload (pinned) + ol_tree_build + ol_search_multi (8 patterns) + "
-                       "ol_doc_read_offsets/kinds + ol_tree_read (4 arrays), on `workers` contexts at once"}
+                       "ol_doc_read_offsets/kinds + ol_tree_read (4 arrays), on `workers` contexts at once, "
+                       "one upload and one download in flight at a time"}
 
     cpu = None
     if rank == 0 and not args.no_cpu:
