@@ -266,19 +266,24 @@ __global__ void __launch_bounds__(DM_THREADS) dict_match_kernel(DictMatchArgs a)
         }
         __syncwarp();
         if (H) {
-            // transpose: word w of heavy pattern h = ballot over positions 32w..32w+31 of bit h
+            // transpose: word w of heavy pattern h holds bit h of positions
+            // 32w..32w+31. Lane q has position 32w+q's mask (a row of a 32x32
+            // bit matrix); five butterfly rounds swap ever smaller off-diagonal
+            // blocks between lanes, after which lane h holds column h.
             uint32_t words[DM_SLICE_WORDS];
 #pragma unroll
             for (uint32_t w = 0; w < DM_SLICE_WORDS; w++) {
-                const uint32_t m = hmask[w * 32 + lane];
-                uint32_t present = __reduce_or_sync(0xFFFFFFFFu, m);
-                words[w] = 0;
-                while (present) {
-                    const uint32_t h = __ffs(present) - 1;
-                    present &= present - 1;
-                    const uint32_t b = __ballot_sync(0xFFFFFFFFu, (m >> h) & 1u);
-                    if (lane == h) words[w] = b;
+                uint32_t x = hmask[w * 32 + lane];
+                if (__any_sync(0xFFFFFFFFu, x != 0)) {
+#pragma unroll
+                    for (uint32_t j = 16; j > 0; j >>= 1) {
+                        const uint32_t left = j == 16 ? 0x0000FFFFu : j == 8 ? 0x00FF00FFu : j == 4 ? 0x0F0F0F0Fu
+                                              : j == 2 ? 0x33333333u : 0x55555555u;  // bits i with (i & j) == 0
+                        const uint32_t y = __shfl_xor_sync(0xFFFFFFFFu, x, j);
+                        x = (lane & j) ? (x & ~left) | ((y & ~left) >> j) : (x & left) | ((y & left) << j);
+                    }
                 }
+                words[w] = x;
             }
             // lane h stores heavy pattern h's words of the slice (contiguous, 16-byte stores)
             if (lane < H) {
