@@ -147,6 +147,45 @@ __device__ __forceinline__ uint32_t dict_walk(const DictMatchArgs &a, const uint
                          ((uint32_t)text[p + 3] << 24);
     uint32_t v = pos + kDictMinLen <= lim ? dict_probe(a.set, key) : NONE;
     uint32_t d = kDictMinLen, hm = 0;
+    if (v != NONE && a.n_chains && key == (key & 0xFFu) * 0x01010101u) {
+        // The position starts a run of one byte c: if c has a chain, jump to
+        // the chain node of depth D = min(run, chain, max length, document
+        // end), taking every pattern c^4..c^D at once, then walk on from it.
+        const uint32_t c = key & 0xFFu;
+        uint32_t j = 0;
+        while (j < a.n_chains && ((a.chain_bytes >> (8 * j)) & 0xFFu) != c) j++;
+        if (j < a.n_chains) {
+            const DictChain *ch = a.chains + j;
+            uint32_t cap = min(__ldg(&ch->K), kDictMaxLen);
+            if (lim - pos < cap) cap = (uint32_t)(lim - pos);  // >= kDictMinLen: the probe ran
+            const uint32_t *tw = reinterpret_cast<const uint32_t *>(text);
+            const uint32_t C4 = c * 0x01010101u;
+            uint32_t run = kDictMinLen;
+            while (run < cap) {  // 4 bytes per step; the staged halo covers p + 67
+                const uint32_t q = p + run;
+                const uint32_t w = __funnelshift_r(tw[q >> 2], tw[(q >> 2) + 1], (q & 3) * 8);
+                const uint32_t z = zero_bytes(w ^ C4);
+                if (z == 0x80808080u) {
+                    run += 4;
+                    continue;
+                }
+                run += (__ffs(~z & 0x80808080u) - 8) >> 3;
+                break;
+            }
+            const uint32_t D = min(run, cap);
+            levels++;
+            hm = __ldg(&ch->cum[D]);
+            const uint32_t nl = __ldg(&ch->n_light);
+            for (uint32_t i = 0; i < nl; i++) {
+                const uint32_t e = __ldg(&ch->light[i]);
+                if ((e >> 24) > D) break;
+                dict_emit(a, hm, e & 0xFFFFFFu, pos);
+            }
+            if (D >= kDictMaxLen || pos + D >= lim) return hm;
+            v = dict_child(a.set, __ldg(a.set.nodes + __ldg(&ch->node[D])), text[p + D]);
+            d = D + 1;
+        }
+    }
     while (v != NONE) {
         const uint4 nd = __ldg(a.set.nodes + v);
         levels++;

@@ -91,7 +91,7 @@ constexpr uint32_t kSearchMaxPatterns = 8;  // patterns per launch
 // parameters.
 struct SearchPatMeta {
     uint32_t pre[4];  // bytes 0..3, each replicated into a word (0 past the end)
-    uint32_t anc[4];  // anchor words (len >= 7): bytes [r, r + 4) little-endian, r = 0..3
+    uint32_t anc[4];  // anchor words (len >= 8): bytes [r, r + 4) little-endian, r = 1..4
     uint32_t len;
     uint32_t f4;      // byte 0 replicated
 };
@@ -117,7 +117,7 @@ struct SearchArgs {
     uint8_t *overflow;
     uint32_t stage_cap;
     SearchPatMeta meta[kSearchMaxPatterns];
-    uint32_t anchor_hash[kSearchMaxPatterns * 4];  // anchor-map bits of the patterns of >= 7 bytes
+    uint32_t anchor_hash[kSearchMaxPatterns * 4];  // anchor-map bits of the patterns of >= 8 bytes
     uint32_t n_anchor;
 };
 constexpr uint32_t kSearchStageCap = 8192;  // staged hits per tile (all patterns of a launch)
@@ -185,6 +185,19 @@ struct DictSet {
 constexpr uint32_t kDictDenseMin = 8;
 constexpr uint32_t kDictDenseFlag = 0x80000000u;
 
+// A byte run in the trie: the path c^4, c^5, ..., c^K (K <= kDictMaxLen) of
+// one byte c, built per search. A walk that starts inside a run of c jumps to
+// the deepest chain node its run reaches: the heavy patterns on the way are
+// one mask, the light ones a short list.
+constexpr uint32_t kDictMaxChains = 4;
+constexpr uint32_t kDictChainMin = 8;  // shorter chains are walked node by node
+struct DictChain {
+    uint32_t byte, K, n_light, pad;
+    uint32_t node[kDictMaxLen + 1];   // trie node of c^d, d = 4..K
+    uint32_t cum[kDictMaxLen + 1];    // heavy bits of the patterns c^4 .. c^d
+    uint32_t light[kDictMaxLen + 1];  // (d << 24) | u of the light patterns on the chain, d ascending
+};
+
 struct DictMatchArgs {
     DictSet set;
     const uint8_t *text;     // padded like every resident text
@@ -206,6 +219,11 @@ struct DictMatchArgs {
     const unsigned long long *seg_end;
     uint32_t n_seg;
     unsigned long long *stats;  // optional: += candidates walked, trie nodes visited
+    // Byte-run chains (not in count mode): n_chains of them, their bytes
+    // packed in chain_bytes (byte j = chain j's byte).
+    const DictChain *chains;
+    uint32_t n_chains;
+    uint32_t chain_bytes;
 };
 
 cudaError_t launch_dict_match(const DictMatchArgs &a, int sm_count, cudaStream_t st, uint32_t slice = 512,

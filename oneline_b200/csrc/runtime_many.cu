@@ -16,12 +16,21 @@
 
 using namespace ol;
 
+// The trie path of a run of one byte, as compiled: node and unique pattern
+// (or NONE) at each depth 4..K.
+struct DictRunPath {
+    uint32_t byte = 0, K = 0;
+    uint32_t node[ol::kDictMaxLen + 1] = {};
+    uint32_t u[ol::kDictMaxLen + 1] = {};
+};
+
 struct ol_patset {
     ol_ctx *ctx = nullptr;
     uint32_t n_ids = 0, n_u = 0, n_nodes = 0;
     DevBuf blob;
     DictSet dev{};
     const uint32_t *u_of_id = nullptr, *dup_start = nullptr, *dup_ids = nullptr;
+    std::vector<DictRunPath> runs;  // the longest byte runs (at most kDictMaxChains)
 };
 
 namespace {
@@ -45,6 +54,7 @@ struct ManyScratch {
     uint32_t *light_n, *error, *id_counts, *sort_hist, *sort_totals;
     uint8_t *heavy_of_u;
     unsigned long long *id_base, *total, *stats;
+    DictChain *chains;
 };
 
 }  // namespace
@@ -128,6 +138,34 @@ extern "C" ol_status ol_patset_compile(ol_ctx *ctx, const ol_doc *doc, const uin
     if (extra.empty()) extra.push_back(0);
     if (dense.empty()) dense.push_back(NONE);
 
+    // Byte runs: the trie path c^4, c^5, ... of each byte c that starts a
+    // pattern with c^4; the longest ones (at least kDictChainMin deep) let
+    // walks inside long runs of c skip down the path (dict_walk).
+    std::vector<DictRunPath> runs;
+    for (uint32_t c = 0; c < 256; c++) {
+        auto it = key_node.find(c * 0x01010101u);
+        if (it == key_node.end()) continue;
+        DictRunPath r;
+        r.byte = c;
+        uint32_t v = it->second, d = kDictMinLen;
+        r.node[d] = v;
+        r.u[d] = trie[v].out;
+        while (d < kDictMaxLen) {
+            uint32_t next = NONE;
+            for (auto &k : trie[v].kids)
+                if (k.first == c) next = k.second;
+            if (next == NONE) break;
+            v = next;
+            d++;
+            r.node[d] = v;
+            r.u[d] = trie[v].out;
+        }
+        r.K = d;
+        if (r.K >= kDictChainMin) runs.push_back(r);
+    }
+    std::sort(runs.begin(), runs.end(), [](const DictRunPath &x, const DictRunPath &y) { return x.K > y.K; });
+    if (runs.size() > kDictMaxChains) runs.resize(kDictMaxChains);
+
     // Filter and hash table over the distinct first-four-byte keys.
     std::vector<uint32_t> filter(1u << (kDictFilterBits - 5), 0);
     uint32_t table_bits = 10;
@@ -204,6 +242,7 @@ extern "C" ol_status ol_patset_compile(ol_ctx *ctx, const ol_doc *doc, const uin
     s->u_of_id = (const uint32_t *)(b + off_uid);
     s->dup_start = (const uint32_t *)(b + off_ds);
     s->dup_ids = (const uint32_t *)(b + off_di);
+    s->runs = std::move(runs);
     *out = s;
     return OL_OK;
 }
@@ -250,6 +289,7 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
     size_t o_hcounts = carve(at, (size_t)kDictMaxHeavy * hld * 4), o_hbases = carve(at, (size_t)kDictMaxHeavy * hld * 4);
     size_t o_ln = carve(at, 16), o_idc = carve(at, (size_t)n * 4), o_idb = carve(at, (size_t)n * 8), o_tot = carve(at, 16);
     size_t o_stot = carve(at, 256 * 4), o_stats = carve(at, 16);
+    size_t o_chains = carve(at, kDictMaxChains * sizeof(DictChain));
     const size_t fixed = at;
     cudaError_t e = ctx->dict_small.reserve(fixed, st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "search_many");
@@ -270,6 +310,7 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
         m.total = (unsigned long long *)(b + o_tot);
         m.sort_totals = (uint32_t *)(b + o_stot);
         m.stats = (unsigned long long *)(b + o_stats);
+        m.chains = (DictChain *)(b + o_chains);
         m.sort_hist = (uint32_t *)(b + fixed);
         return m;
     };
@@ -324,7 +365,33 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
         heavy_u[h] = cand[h].second;
         heavy_of[cand[h].second] = (uint8_t)h;
     }
+    // The byte-run chains of this search: heavy bits accumulated down each run,
+    // and its light patterns.
+    std::vector<DictChain> chains(set->runs.size());
+    uint32_t chain_bytes = 0;
+    for (size_t j = 0; j < set->runs.size(); j++) {
+        const DictRunPath &r = set->runs[j];
+        DictChain &c = chains[j];
+        memset(&c, 0, sizeof c);
+        c.byte = r.byte;
+        c.K = r.K;
+        chain_bytes |= r.byte << (8 * j);
+        uint32_t acc = 0;
+        for (uint32_t dd = kDictMinLen; dd <= r.K; dd++) {
+            c.node[dd] = r.node[dd];
+            const uint32_t u = r.u[dd];
+            if (u != NONE) {
+                if (heavy_of[u] != 0xFF)
+                    acc |= 1u << heavy_of[u];
+                else
+                    c.light[c.n_light++] = (dd << 24) | u;
+            }
+            c.cum[dd] = acc;
+        }
+    }
     e = cudaMemcpyAsync(m.heavy_of_u, heavy_of.data(), U, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !chains.empty())
+        e = cudaMemcpyAsync(m.chains, chains.data(), chains.size() * sizeof(DictChain), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(m.heavy_u, heavy_u.data(), kDictMaxHeavy * 4, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && H) e = ctx->dict_bitmap.reserve((size_t)H * n_words * 4, st);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "search_many");
@@ -347,6 +414,9 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
         ma.light_keys = (unsigned long long *)ctx->dict_keys.ptr;
         ma.light_cap = (uint32_t)cap;
         ma.light_n = m.light_n;
+        ma.chains = m.chains;
+        ma.n_chains = (uint32_t)chains.size();
+        ma.chain_bytes = chain_bytes;
         if (e == cudaSuccess) e = launch_dict_match(ma, ctx->sm_count, st, ctx->tune.dict_slice, ctx->tune.dict_blocks_per_sm);
         if (e == cudaSuccess) e = cudaMemcpyAsync(flags, m.light_n, 8, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);

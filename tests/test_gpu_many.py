@@ -123,3 +123,26 @@ def test_limits_errors_and_empty_document(parser):
     assert r.total_hits == 0 and r.counts.tolist() == [0, 0]
     r = parser.search_many(parser.upload(b"abc"), ps, 10)
     assert r.total_hits == 0
+
+
+@pytest.mark.parametrize("heavy_min_hits", [1, 200, 1 << 30])
+def test_runs_of_one_byte(parser, heavy_min_hits):
+    """Walks that start inside long runs of one byte jump down the trie path of
+    that run: patterns c^4..c^64 (some missing, some duplicated, some longer
+    than the run), patterns that continue a run with another byte, runs of
+    every length from 1 to 90, and runs cut by the text end. Every hit equals
+    the oracle's, with all, some or none of the run patterns heavy."""
+    rng = np.random.default_rng(7)
+    parts = []
+    for n in list(range(1, 91)) * 3:
+        c = b"|" if rng.random() < 0.7 else b"-"
+        parts.append(c * int(n))
+        parts.append(bytes(rng.integers(97, 123, size=int(rng.integers(1, 6)), dtype=np.uint8)))
+    text = b"".join(parts) + b"|" * 37
+    pats = [b"|" * k for k in range(4, 65) if k % 7 != 3]
+    pats += [b"-" * k for k in (4, 5, 8, 13, 21, 34, 55)]
+    pats += [b"|" * 9, b"|" * 9]  # duplicated ids
+    pats += [b"|" * k + b"a" for k in (3, 4, 6, 10, 20, 40, 63)]
+    pats += [b"|" * k + b"-" for k in (4, 12)] + [b"a|||", b"||||a|||"]
+    assert_many_device(parser, text, pats, heavy_min_hits, what=f"heavy >= {heavy_min_hits}")
+    assert_many(parser, text, pats, what="host hits")
