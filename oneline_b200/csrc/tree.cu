@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(1024) tree_scan_kernel(TreeArgs a) {
 // the stack of the lines after them, walks forward for parent (and the
 // parent's depth, kept in registers) and backward for subtree_end,
 // first_child and next_sibling.
-__global__ void __launch_bounds__(TR_THREADS) tree_resolve_kernel(TreeArgs a) {
+__global__ void __launch_bounds__(TR_THREADS, 5) tree_resolve_kernel(TreeArgs a) {
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, tile = blockIdx.x;
     const uint32_t D = a.levels;
     TreeSmem sm = tree_smem(D);
