@@ -116,6 +116,8 @@ struct SearchArgs {
     uint16_t *stage;
     uint8_t *overflow;
     uint32_t stage_cap;
+    uint32_t *overflow_n;     // staged form: count, then list, of the flagged tiles (n_tiles entries)
+    uint32_t *overflow_list;
     SearchPatMeta meta[kSearchMaxPatterns];
     uint32_t anchor_hash[kSearchMaxPatterns * 4];  // anchor-map bits of the patterns of >= 8 bytes
     uint32_t n_anchor;

@@ -73,8 +73,11 @@ cudaError_t ol::launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const 
     const size_t col_words = (size_t)scan_ld(n_tiles) * kSearchMaxPatterns;  // counts, then bases
     cudaError_t e = ctx->scratch_a.reserve(col_words * 4 * 2, st);
     // staging: kSearchStageCap tile offsets per tile, then the overflow flags
+    // then the flagged tiles' count and list
     const size_t stage_bytes = (size_t)n_tiles * kSearchStageCap * 2;
-    if (e == cudaSuccess && ctx->tune.search_staged) e = ctx->search_stage.reserve(stage_bytes + n_tiles + 16, st);
+    const size_t list_at = (stage_bytes + n_tiles + 15) & ~size_t(15);
+    if (e == cudaSuccess && ctx->tune.search_staged)
+        e = ctx->search_stage.reserve(list_at + 16 + (size_t)n_tiles * 4, st);
     if (e != cudaSuccess) return e;
     uint32_t i = 0;
     while (i < n) {
@@ -87,6 +90,8 @@ cudaError_t ol::launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const 
         a.bases = (uint32_t *)ctx->scratch_a.ptr + col_words;
         a.stage = ctx->tune.search_staged ? (uint16_t *)ctx->search_stage.ptr : nullptr;
         a.overflow = (uint8_t *)ctx->search_stage.ptr + stage_bytes;
+        a.overflow_n = (uint32_t *)((uint8_t *)ctx->search_stage.ptr + list_at);
+        a.overflow_list = a.overflow_n + 4;
         a.stage_cap = kSearchStageCap;
         uint32_t halo = 0;
         bool alone = halo_for(lens[i]) > kSearchMaxStagedPattern;

@@ -29,6 +29,8 @@
 // (4-byte window filter, slot atomics, host sort).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "ol_common.cuh"
 #include "ol_kernels.h"
 
@@ -354,14 +356,10 @@ __global__ void __launch_bounds__(SR_THREADS) search_count_kernel(SearchArgs a) 
 // thread writes its matches there: the block's stores cover one contiguous
 // range. Tiles without matches exit before loading text.
 template <uint32_t NP>
-__global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) {
-    __shared__ SearchSmem sm;
-    __shared__ uint16_t match[NP][SR_PIECES];
-    __shared__ uint32_t warp_sum[SR_THREADS / 32];
+__device__ __forceinline__ void write_tile(const SearchArgs &a, SearchSmem &sm, uint16_t (*match)[SR_PIECES],
+                                           uint32_t *warp_sum, uint32_t tile) {
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t tile = blockIdx.x;
     const uint64_t t0 = (uint64_t)tile * kSearchTile;
-    if (a.stage && !a.overflow[tile]) return;  // written from the staged hits
     // patterns with matches here whose output window is not yet full
     uint32_t want = 0;
     for (uint32_t p = 0; p < NP; p++) {
@@ -405,6 +403,21 @@ __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) 
         }
         __syncthreads();  // warp_sum is reused by the next pattern
     }
+}
+
+// Recomputing form: block b writes tile b. Staged form: a small grid takes
+// the tiles the stage pass listed as overflowing their slots (usually none).
+template <uint32_t NP>
+__global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) {
+    __shared__ SearchSmem sm;
+    __shared__ uint16_t match[NP][SR_PIECES];
+    __shared__ uint32_t warp_sum[SR_THREADS / 32];
+    if (!a.stage) {
+        write_tile<NP>(a, sm, match, warp_sum, blockIdx.x);
+        return;
+    }
+    const uint32_t n = *a.overflow_n;
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) write_tile<NP>(a, sm, match, warp_sum, a.overflow_list[i]);
 }
 
 // ----------------------------------------------------------- staged path --
@@ -511,7 +524,10 @@ __global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) 
         if (tid == 0) a.counts[(size_t)p * a.ld + tile] = tot;
         start += tot;
     }
-    if (tid == 0) a.overflow[tile] = start > a.stage_cap ? 1 : 0;
+    if (tid == 0) {
+        a.overflow[tile] = start > a.stage_cap ? 1 : 0;
+        if (start > a.stage_cap) a.overflow_list[atomicAdd(a.overflow_n, 1u)] = tile;
+    }
     if (start > a.stage_cap) return;  // uniform: recomputed later
     __syncthreads();
     uint4 *dst = reinterpret_cast<uint4 *>(a.stage + (size_t)tile * a.stage_cap);
@@ -589,14 +605,18 @@ void search_add_pattern(SearchArgs &a, const uint8_t *host, const uint8_t *dev, 
         }
 }
 
+constexpr uint32_t kSearchWriteGrid = 512;  // blocks of the staged form's write pass
+
 template <uint32_t NP>
 static cudaError_t launch_search_np(const SearchArgs &a, cudaStream_t st) {
     if (a.stage) {
+        cudaError_t e0 = cudaMemsetAsync(a.overflow_n, 0, sizeof(uint32_t), st);
+        if (e0 != cudaSuccess) return e0;
         search_stage_kernel<NP><<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
         cudaError_t e = launch_scan_columns(a.counts, a.bases, a.totals, a.n_tiles, a.np, a.ld, st);
         if (e != cudaSuccess) return e;
         search_copy_kernel<<<(a.n_tiles + SC_TILES - 1) / SC_TILES, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
-        search_write_kernel<NP><<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();  // flagged tiles only
+        search_write_kernel<NP><<<std::min(a.n_tiles, kSearchWriteGrid), SR_THREADS, 0, st>>>(a); OL_LAUNCHED();  // listed tiles
         return cudaGetLastError();
     }
     search_count_kernel<NP><<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();

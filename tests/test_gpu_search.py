@@ -174,3 +174,25 @@ def test_patterns_ending_in_nul_do_not_match_the_padding(parser):
         res = parser.search_document_multi(doc, pats, 4)
         for p, w, r in zip(pats, want, res):
             assert r.total_matches == len(w) and np.array_equal(r.offsets, w), p
+
+
+def test_tiles_whose_hits_overflow_the_staging_slot(parser):
+    """A tile with more hits than its staging slot holds (8192 for all the
+    patterns of a pass) is recomputed in place; the others are copied from
+    their slots. Dense runs of one byte put 16,384 hits in a tile."""
+    rng = np.random.default_rng(3)
+    parts = []
+    for i in range(12):
+        parts.append(b"a" * int(rng.integers(10_000, 40_000)))
+        parts.append(bytes(rng.integers(98, 123, size=int(rng.integers(1_000, 30_000)), dtype=np.uint8)))
+    text = b"".join(parts)
+    pats = [b"a", b"aa", b"aaaa", b"aaaaaaaaa", b"ab", b"b", b"zz", b"a" * 40]
+    doc = parser.upload(text)
+    want = [oracle.find_all(text, p) for p in pats]
+    for group in (pats[:1], pats[:3], pats):
+        res = parser.search_document_multi(doc, group, [len(w) for w in want[:len(group)]])
+        for p, w, r in zip(group, want, res):
+            assert r.total_matches == len(w) and np.array_equal(r.offsets, w), (len(group), p)
+    res = parser.search_document_multi(doc, pats, 1000)  # truncated: the lowest 1000 of each
+    for p, w, r in zip(pats, want, res):
+        assert r.total_matches == len(w) and np.array_equal(r.offsets, w[:1000]), p
