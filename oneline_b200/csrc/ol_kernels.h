@@ -33,7 +33,16 @@ struct ParseArgs {
     uint32_t line_cap;
     uint2 *fixup;           // (line index, start) of lines longer than the halo
     uint32_t fixup_cap;
+    // Staged form (nullptr: count pass + recomputing pass): per tile a slot of
+    // slot_cap line words, a flag per tile whose lines did not fit, and the
+    // count and list of those tiles.
+    uint32_t *slot;
+    uint8_t *slot_over;
+    uint32_t *redo_n;
+    uint32_t *redo_list;
+    uint32_t slot_cap;
 };
+constexpr uint32_t kParseSlotCap = 1024;  // staged lines per tile
 
 cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st);
 

@@ -20,6 +20,8 @@
 // starts) and crates/oneline-simd/src/line.rs:8-81 (classification).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "ol_common.cuh"
 #include "ol_kernels.h"
 
@@ -39,7 +41,16 @@ struct ParseSmem {
     uint32_t warp_tot[PT_STEPS][8];  // newline count per (step, warp)
     uint32_t warp_base[PT_STEPS][8];
     uint32_t halo_first;             // first newline in the halo (local), or NONE
+    uint32_t tile_nl;                // newlines in the tile
 };
+
+// Staged form: a tile's lines as one word each, (start, kind, depth8) or a
+// marker, in its slot of PT_LIST words.
+constexpr uint32_t kSlotNone = 0xFFFFFFFFu;  // a final '\n' that starts no line
+constexpr uint32_t kSlotFixup = 1u << 26;    // the line runs past the halo: the fix-up kernel classifies it
+__device__ __forceinline__ uint32_t slot_word(uint32_t s, uint32_t kind, uint32_t depth) {
+    return s | (kind << 15) | (min(depth, 255u) << 18);  // s <= 16384: 15 bits
+}
 
 // 4 bytes of shared memory from any byte offset.
 __device__ __forceinline__ uint32_t lds4(const uint8_t *base, uint32_t off) {
@@ -138,16 +149,19 @@ __global__ void __launch_bounds__(PT_THREADS) newline_count_kernel(const uint8_t
     }
 }
 
-// Pass 3: CTA b re-reads tile b, lists its newlines in position order (warp
-// popc scans) and classifies every line that starts after one of them (plus
-// line 0 for tile 0) from shared memory, knowing the tile's first line index
-// from the scan of pass 2. Consecutive threads take consecutive lines, so the
-// outputs are written coalesced. A line that runs past the tile plus a
-// 256-byte halo is queued for the fix-up kernel.
-__global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a) {
-    __shared__ ParseSmem sm;
+// One tile: the block loads tile b, lists its newlines in position order
+// (warp popc scans) and classifies every line that starts after one of them
+// (plus line 0 for tile 0) from shared memory. Consecutive threads take
+// consecutive lines. A line that runs past the tile plus a 256-byte halo is
+// left to the fix-up kernel.
+//   STAGE: the tile's newline count goes to tile_count and its lines, by
+//     tile-local rank, to its slot (a tile with more lines than a slot holds
+//     is listed for the recomputing form instead);
+//   else: the tile's first line index comes from tile_base (the scan of the
+//     counts), and offsets, kinds and depth8 are written in place.
+template <bool STAGE>
+__device__ __forceinline__ void parse_tile(const ParseArgs &a, ParseSmem &sm, uint32_t tile) {
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t tile = blockIdx.x;
     const uint64_t t0 = (uint64_t)tile * PT_TILE;
     const uint64_t N = a.text_len;
     // bytes of this tile (and halo) that belong to the text
@@ -215,16 +229,31 @@ __global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a)
             if ((int)lane >= o) inc += t;
         }
         sm.warp_base[lane >> 3][lane & 7] = inc - c;
+        if (lane == 31) sm.tile_nl = inc;
     }
     __syncthreads();  // (b) bases and halo_first visible
 
-    const uint32_t nl_base = a.tile_base[tile];  // newlines before this tile
-    const uint32_t n_nl = a.tile_count[tile];
     const uint32_t off = tile == 0 ? 1u : 0u;
+    uint32_t nl_base, n_nl;
+    if (STAGE) {
+        n_nl = sm.tile_nl;
+        nl_base = 0;
+        const bool over = n_nl + off > a.slot_cap;
+        if (tid == 0) {
+            a.tile_count[tile] = n_nl;
+            a.slot_over[tile] = over ? 1 : 0;
+            if (over) a.redo_list[atomicAdd(a.redo_n, 1u)] = tile;
+        }
+        if (over) return;  // uniform
+    } else {
+        nl_base = a.tile_base[tile];  // newlines before this tile
+        n_nl = a.tile_count[tile];
+        if (tile == a.n_tiles - 1 && tid == 0)  // L = 1 + newlines before the last byte
+            a.stats->line_count = 1u + nl_base + n_nl - (a.text[N - 1] == '\n');
+    }
     const uint32_t n_lines = n_nl + off;
     const uint32_t halo_first = sm.halo_first;
-    if (tile == a.n_tiles - 1 && tid == 0)  // L = 1 + newlines before the last byte
-        a.stats->line_count = 1u + nl_base + n_nl - (a.text[N - 1] == '\n');
+    uint32_t *slot = STAGE ? a.slot + (size_t)tile * a.slot_cap : nullptr;
     uint32_t my_max = 0;
 
     // Lines are classified in rounds of PT_LIST (one round unless the tile
@@ -253,34 +282,106 @@ __global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a)
         for (uint32_t j = r0 + tid; j < r_end; j += PT_THREADS) {
             int32_t q = (int32_t)j - (int32_t)off;  // newline that precedes the line (-1: none)
             uint32_t s = q < 0 ? 0u : sm.nl[q - w0] + 1u;  // tile-local
-            if (s >= valid) continue;  // the final '\n' starts no line
-            uint32_t idx = nl_base + j + 1 - off;
-            if (idx >= a.line_cap) {
-                atomicOr(&a.stats->error, OL_DEVERR_CAPACITY);
+            if (s >= valid) {  // the final '\n' starts no line
+                if (STAGE) slot[j] = kSlotNone;
                 continue;
             }
-            a.offsets[idx] = (uint32_t)t0 + s;
+            uint32_t idx = nl_base + j + 1 - off;
+            if (!STAGE) {
+                if (idx >= a.line_cap) {
+                    atomicOr(&a.stats->error, OL_DEVERR_CAPACITY);
+                    continue;
+                }
+                a.offsets[idx] = (uint32_t)t0 + s;
+            }
             uint32_t e;
             if ((uint32_t)(q + 1) < n_nl) e = sm.nl[q + 1 - w0];
             else if (halo_first != NONE) e = halo_first;
             else if (valid < PT_TILE + PT_HALO) e = valid;  // the text ends in the staged bytes
             else {
                 // runs past the halo: classified by the fix-up kernel
-                uint32_t slot = atomicAdd(&a.stats->fixup_count, 1u);
-                if (slot < a.fixup_cap) a.fixup[slot] = make_uint2(idx, (uint32_t)t0 + s);
-                else atomicOr(&a.stats->error, OL_DEVERR_FIXUP);
+                if (STAGE) {
+                    slot[j] = s | kSlotFixup;
+                } else {
+                    uint32_t fx = atomicAdd(&a.stats->fixup_count, 1u);
+                    if (fx < a.fixup_cap) a.fixup[fx] = make_uint2(idx, (uint32_t)t0 + s);
+                    else atomicOr(&a.stats->error, OL_DEVERR_FIXUP);
+                }
                 continue;
             }
             uint32_t depth;
             uint32_t kind = classify_smem(sm.text, s, e, depth);
-            a.kinds[idx] = (uint8_t)kind;
-            a.depth8[idx] = (uint8_t)min(depth, 255u);
+            if (STAGE) {
+                slot[j] = slot_word(s, kind, depth);
+            } else {
+                a.kinds[idx] = (uint8_t)kind;
+                a.depth8[idx] = (uint8_t)min(depth, 255u);
+            }
             if (kind != KIND_BLANK) my_max = max(my_max, depth);
         }
         __syncthreads();  // (d) the next round may overwrite the list
     }
     for (int o = 16; o > 0; o >>= 1) my_max = max(my_max, __shfl_xor_sync(0xFFFFFFFFu, my_max, o));
     if (lane == 0 && my_max) atomicMax(&a.stats->max_content_depth, my_max);
+}
+
+// Recomputing form, every tile (pass 3 after newline_count_kernel and the scan).
+__global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a) {
+    __shared__ ParseSmem sm;
+    parse_tile<false>(a, sm, blockIdx.x);
+}
+
+// Staged form, pass 1: every tile counts its newlines and stages its lines.
+__global__ void __launch_bounds__(PT_THREADS, 6) parse_stage_kernel(ParseArgs a) {
+    __shared__ ParseSmem sm;
+    parse_tile<true>(a, sm, blockIdx.x);
+}
+
+// Staged form, pass 3: the tiles listed by pass 1 (more lines than a slot
+// holds) in the recomputing form, now that their first line index is known.
+__global__ void __launch_bounds__(PT_THREADS, 6) parse_redo_kernel(ParseArgs a) {
+    __shared__ ParseSmem sm;
+    const uint32_t n = *a.redo_n;
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        parse_tile<false>(a, sm, a.redo_list[i]);
+        __syncthreads();  // shared memory is reused by the next tile
+    }
+}
+
+// Staged form, pass 2: one warp per tile writes its staged lines at their
+// line indices (the scan of the counts): offsets, kinds and depth8, or a
+// fix-up entry for a line that runs past the halo.
+constexpr uint32_t PC_TILES = 8;  // tiles per block
+__global__ void __launch_bounds__(256) parse_copy_kernel(ParseArgs a) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t tile = blockIdx.x * PC_TILES + (threadIdx.x >> 5);
+    if (tile >= a.n_tiles || a.slot_over[tile]) return;
+    const uint32_t off = tile == 0 ? 1u : 0u;
+    const uint32_t n_nl = a.tile_count[tile], nl_base = a.tile_base[tile];
+    const uint32_t n_lines = n_nl + off;
+    const uint32_t t0 = tile * PT_TILE;
+    if (tile == a.n_tiles - 1 && lane == 0)  // L = 1 + newlines before the last byte
+        a.stats->line_count = 1u + nl_base + n_nl - (a.text[a.text_len - 1] == '\n');
+    const uint32_t *slot = a.slot + (size_t)tile * a.slot_cap;
+    for (uint32_t j = lane; j < n_lines; j += 32) {
+        const uint32_t w = slot[j];
+        if (w == kSlotNone) continue;
+        const uint32_t idx = nl_base + j + 1 - off;
+        if (idx >= a.line_cap) {
+            atomicOr(&a.stats->error, OL_DEVERR_CAPACITY);
+            continue;
+        }
+        const uint32_t s = t0 + (w & 0x7FFFu);
+        a.offsets[idx] = s;
+        if (w & kSlotFixup) {
+            const uint32_t fx = atomicAdd(&a.stats->fixup_count, 1u);
+            if (fx < a.fixup_cap) a.fixup[fx] = make_uint2(idx, s);
+            else atomicOr(&a.stats->error, OL_DEVERR_FIXUP);
+            continue;
+        }
+        a.kinds[idx] = (uint8_t)((w >> 15) & 7u);
+        a.depth8[idx] = (uint8_t)((w >> 18) & 0xFFu);
+    }
 }
 
 // Lines queued by the tile kernel: their end comes from the complete offsets
@@ -327,10 +428,22 @@ __global__ void classify_lines_kernel(const uint8_t *__restrict__ text, uint64_t
 
 cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st) {
     if (a.n_tiles == 0) return cudaSuccess;
-    newline_count_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a.text, a.text_len, a.tile_count); OL_LAUNCHED();
-    cudaError_t e = launch_scan_columns(a.tile_count, a.tile_base, nullptr, a.n_tiles, 1, scan_ld(a.n_tiles), st);
-    if (e != cudaSuccess) return e;
-    parse_tiles_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a); OL_LAUNCHED();
+    cudaError_t e;
+    if (a.slot) {
+        // staged: the text is read once; tiles with too many lines are redone
+        if (a.slot_cap > PT_LIST) return cudaErrorInvalidValue;  // a slot is listed in one round
+        if ((e = cudaMemsetAsync(a.redo_n, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+        parse_stage_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a); OL_LAUNCHED();
+        e = launch_scan_columns(a.tile_count, a.tile_base, nullptr, a.n_tiles, 1, scan_ld(a.n_tiles), st);
+        if (e != cudaSuccess) return e;
+        parse_copy_kernel<<<(a.n_tiles + PC_TILES - 1) / PC_TILES, 256, 0, st>>>(a); OL_LAUNCHED();
+        parse_redo_kernel<<<std::min(a.n_tiles, 512u), PT_THREADS, 0, st>>>(a); OL_LAUNCHED();
+    } else {
+        newline_count_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a.text, a.text_len, a.tile_count); OL_LAUNCHED();
+        e = launch_scan_columns(a.tile_count, a.tile_base, nullptr, a.n_tiles, 1, scan_ld(a.n_tiles), st);
+        if (e != cudaSuccess) return e;
+        parse_tiles_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a); OL_LAUNCHED();
+    }
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     uint32_t blocks = a.fixup_cap < 64 ? 8 : 64;

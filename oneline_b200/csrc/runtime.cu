@@ -138,6 +138,7 @@ extern "C" void ol_ctx_destroy(ol_ctx *ctx) {
     ctx->scratch_a.release(ctx->stream);
     ctx->scratch_b.release(ctx->stream);
     ctx->scratch_c.release(ctx->stream);
+    ctx->parse_slot.release(ctx->stream);
     ctx->search_out.release(ctx->stream);
     ctx->search_stage.release(ctx->stream);
     ctx->pattern_dev.release(ctx->stream);
@@ -219,6 +220,16 @@ cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d) {
     a.line_cap = d->line_cap;
     a.fixup = d->fixup;
     a.fixup_cap = n_tiles;
+    // staged form: slots, then the per-tile flags, then the redo count and list
+    const size_t slot_bytes = (size_t)n_tiles * kParseSlotCap * 4;
+    const size_t list_at = (slot_bytes + n_tiles + 15) & ~size_t(15);
+    if ((e = ctx->parse_slot.reserve(list_at + 16 + (size_t)n_tiles * 4, st)) != cudaSuccess) return e;
+    uint8_t *ps = (uint8_t *)ctx->parse_slot.ptr;
+    a.slot = (uint32_t *)ps;
+    a.slot_over = ps + slot_bytes;
+    a.redo_n = (uint32_t *)(ps + list_at);
+    a.redo_list = a.redo_n + 4;
+    a.slot_cap = kParseSlotCap;
     return launch_parse(a, st);
 }
 

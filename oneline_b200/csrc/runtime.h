@@ -46,6 +46,7 @@ struct ol_ctx {
     ol::DevBuf scratch_c;  // nodes and other per-call outputs
     ol::DevBuf search_out;
     ol::DevBuf search_stage;  // staged search hits, 16 KiB per text tile
+    ol::DevBuf parse_slot;    // staged parse lines, 4 KiB per text tile
     ol_tuning tune{512, 0, 512, 1};  // kernel variants in use (ol_autotune / ol_tuning_set)
     uint64_t dict_stats[6] = {0, 0, 0, 0, 0, 0};  // the last dictionary search (ol_dict_stats)
     ol::DevBuf pattern_dev;

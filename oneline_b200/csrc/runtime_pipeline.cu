@@ -100,16 +100,16 @@ extern "C" ol_status ol_pipeline_capture(ol_ctx *ctx, ol_doc *d, ol_tree *t, con
     if (e == cudaSuccess) e = enqueue_step(pc, d, t, patterns, dp, ln, max_matches, d_totals, d_outs);
     if (e == cudaSuccess) e = cudaStreamSynchronize(pc->stream);
     p->kernels = (uint32_t)(ol_launch_count() - l0);
-    void *before[6] = {pc->scratch_a.ptr, pc->scratch_b.ptr, pc->scratch_c.ptr, t->parent_buf.ptr, t->end_buf.ptr,
-                       p->patterns.ptr};
+    void *before[8] = {pc->scratch_a.ptr, pc->scratch_b.ptr,   pc->scratch_c.ptr, t->parent_buf.ptr, t->end_buf.ptr,
+                       p->patterns.ptr,   pc->parse_slot.ptr, pc->search_stage.ptr};
     if (e == cudaSuccess) e = cudaStreamBeginCapture(pc->stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
         cudaError_t ce = enqueue_step(pc, d, t, patterns, dp, ln, max_matches, d_totals, d_outs);
         e = cudaStreamEndCapture(pc->stream, &p->graph);
         if (ce != cudaSuccess) e = ce;
     }
-    void *after[6] = {pc->scratch_a.ptr, pc->scratch_b.ptr, pc->scratch_c.ptr, t->parent_buf.ptr, t->end_buf.ptr,
-                      p->patterns.ptr};
+    void *after[8] = {pc->scratch_a.ptr, pc->scratch_b.ptr,   pc->scratch_c.ptr, t->parent_buf.ptr, t->end_buf.ptr,
+                      p->patterns.ptr,   pc->parse_slot.ptr, pc->search_stage.ptr};
     if (e == cudaSuccess && memcmp(before, after, sizeof before) != 0) e = cudaErrorStreamCaptureInvalidated;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
     if (e != cudaSuccess) {

@@ -70,6 +70,18 @@ def test_many_tiles_and_awkward_shapes(parser):
         assert_parse_matches(parser, case, repr(case[:20]))
 
 
+def test_tiles_with_more_lines_than_a_slot(parser):
+    """Tiles of up to 1024 lines are staged and copied; denser tiles (short or
+    empty lines) are parsed again once their first line index is known. Both
+    kinds side by side, the dense runs starting and ending at every offset
+    around a tile edge."""
+    corpus = datagen.corpus(1 << 20, 5).tobytes()
+    for cut in [16384 - 3, 16384, 16384 + 1, 3 * 16384 + 7]:
+        dense = b"\n" * 5000 + b"|\n" * 3000 + b"| -\n" * 2000
+        text = corpus[:cut] + dense + corpus[cut: cut + 100_000] + dense + corpus[:50_000] + b"|" * 17
+        assert_parse_matches(parser, text, f"dense at {cut}")
+
+
 def test_lines_across_tile_and_halo_boundaries(parser):
     """Line ends and prefixes at every distance around the 16 KiB tile and its 256-byte halo."""
     tile = 16384
