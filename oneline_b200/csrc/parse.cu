@@ -363,24 +363,34 @@ __global__ void __launch_bounds__(256) parse_copy_kernel(ParseArgs a) {
     if (tile == a.n_tiles - 1 && lane == 0)  // L = 1 + newlines before the last byte
         a.stats->line_count = 1u + nl_base + n_nl - (a.text[a.text_len - 1] == '\n');
     const uint32_t *slot = a.slot + (size_t)tile * a.slot_cap;
-    for (uint32_t j = lane; j < n_lines; j += 32) {
-        const uint32_t w = slot[j];
-        if (w == kSlotNone) continue;
-        const uint32_t idx = nl_base + j + 1 - off;
-        if (idx >= a.line_cap) {
-            atomicOr(&a.stats->error, OL_DEVERR_CAPACITY);
-            continue;
+    for (uint32_t j0 = 0; j0 < n_lines; j0 += 128) {
+        uint32_t ws[4];  // four independent loads in flight per lane
+#pragma unroll
+        for (uint32_t r = 0; r < 4; r++) {
+            const uint32_t j = j0 + r * 32 + lane;
+            ws[r] = j < n_lines ? __ldg(slot + j) : kSlotNone;
         }
-        const uint32_t s = t0 + (w & 0x7FFFu);
-        a.offsets[idx] = s;
-        if (w & kSlotFixup) {
-            const uint32_t fx = atomicAdd(&a.stats->fixup_count, 1u);
-            if (fx < a.fixup_cap) a.fixup[fx] = make_uint2(idx, s);
-            else atomicOr(&a.stats->error, OL_DEVERR_FIXUP);
-            continue;
+#pragma unroll
+        for (uint32_t r = 0; r < 4; r++) {
+            const uint32_t j = j0 + r * 32 + lane;
+            const uint32_t w = ws[r];
+            if (w == kSlotNone) continue;
+            const uint32_t idx = nl_base + j + 1 - off;
+            if (idx >= a.line_cap) {
+                atomicOr(&a.stats->error, OL_DEVERR_CAPACITY);
+                continue;
+            }
+            const uint32_t s = t0 + (w & 0x7FFFu);
+            a.offsets[idx] = s;
+            if (w & kSlotFixup) {
+                const uint32_t fx = atomicAdd(&a.stats->fixup_count, 1u);
+                if (fx < a.fixup_cap) a.fixup[fx] = make_uint2(idx, s);
+                else atomicOr(&a.stats->error, OL_DEVERR_FIXUP);
+                continue;
+            }
+            a.kinds[idx] = (uint8_t)((w >> 15) & 7u);
+            a.depth8[idx] = (uint8_t)((w >> 18) & 0xFFu);
         }
-        a.kinds[idx] = (uint8_t)((w >> 15) & 7u);
-        a.depth8[idx] = (uint8_t)((w >> 18) & 0xFFu);
     }
 }
 
