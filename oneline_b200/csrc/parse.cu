@@ -1,18 +1,22 @@
 // Kernel (a)+(b): newline scan fused with per-line classification.
 //
-// Three launches, no block ever waits on another:
-//   1. newline_count_kernel: per 16 KiB tile, the newline count (16-byte
-//      coalesced vector loads, exact byte SWAR, popc, warp reductions);
+// Staged form (the default), no block ever waits on another:
+//   1. parse_stage_kernel: per 16 KiB tile, the newline count (16-byte
+//      coalesced vector loads, exact byte SWAR, popc, warp scans), the
+//      newline positions in order, and the classification of every line
+//      starting in the tile from shared memory, staged as one word per line
+//      in the tile's slot;
 //   2. scan_columns_kernel: exclusive scan of the tile counts = every tile's
 //      first line index;
-//   3. parse_tiles_kernel: per tile, the newline positions in order (warp popc
-//      scans) and the classification of every line starting in the tile, from
-//      shared memory, written coalesced at the line indices from step 2.
-// The text is read twice from HBM; a single pass with a decoupled look-back
-// was measured slower here: the look-back chain fell behind the tile rate.
-// A line that runs past the tile plus a 256-byte halo is queued for a small
-// fix-up kernel, which reads it from global memory once the offsets array is
-// complete.
+//   3. parse_copy_kernel: one warp per tile writes the staged lines at their
+//      line indices; parse_redo_kernel parses the tiles with more lines than
+//      a slot holds again, in place.
+// The text is read once. The recomputing form (newline_count_kernel, the
+// scan, parse_tiles_kernel) reads it twice and needs no slots. A single pass
+// with a decoupled look-back was measured slower here: the look-back chain
+// fell behind the tile rate. A line that runs past the tile plus a 256-byte
+// halo is queued for a small fix-up kernel, which reads it from global memory
+// once the offsets array is complete.
 //
 // Replaces crates/oneline-gpu/src/scan.wgsl:20-237 (three passes + a host read
 // of the line count) and shader.wgsl:34-134 (one thread per line, byte loads
