@@ -535,14 +535,15 @@ __global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) 
     for (uint32_t o = tid; o < (start + 7) / 8; o += SR_THREADS) dst[o] = src[o];
 }
 
-// Pass 2 of the staged path: one warp per tile. Lane p reads pattern p's
+// Pass 2 of the staged path: two warps per tile. Lane p reads pattern p's
 // count and first output slot (all patterns at once: one memory round trip),
-// a warp scan places each pattern's hits in the tile's slot, and the warp
-// copies them to their final slots, 32 per step.
-constexpr uint32_t SC_TILES = SR_THREADS / 32;  // tiles per block
+// a warp scan places each pattern's hits in the tile's slot, and the warps
+// copy them to their final slots, alternate runs of 128 each.
+constexpr uint32_t SC_WARPS = 2;                          // warps per tile
+constexpr uint32_t SC_TILES = SR_THREADS / 32 / SC_WARPS;  // tiles per block
 __global__ void __launch_bounds__(SR_THREADS) search_copy_kernel(SearchArgs a) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t tile = blockIdx.x * SC_TILES + (threadIdx.x >> 5);
+    const uint32_t lane = threadIdx.x & 31, half = (threadIdx.x >> 5) % SC_WARPS;
+    const uint32_t tile = blockIdx.x * SC_TILES + (threadIdx.x >> 5) / SC_WARPS;
     if (tile >= a.n_tiles || a.overflow[tile]) return;  // overflowing tiles: search_write_kernel
     uint32_t n = 0, base = 0, max_out = 0;
     if (lane < a.np) {
@@ -568,8 +569,9 @@ __global__ void __launch_bounds__(SR_THREADS) search_copy_kernel(SearchArgs a) {
         const uint32_t lim = b >= mx ? 0u : min(np_, mx - b);  // the first max_out hits overall
         uint32_t *__restrict__ out = a.out[p] + b;
         const uint16_t *__restrict__ src = slot + start;
-        // four independent loads in flight per lane before the stores
-        for (uint32_t i0 = 0; i0 < lim; i0 += 128) {
+        // the tile's warps take alternate runs of 128 hits; four independent
+        // loads in flight per lane before the stores
+        for (uint32_t i0 = half * 128; i0 < lim; i0 += 128 * SC_WARPS) {
             uint32_t v[4];
 #pragma unroll
             for (uint32_t j = 0; j < 4; j++) {
