@@ -194,8 +194,8 @@ __device__ __forceinline__ void load_tile(const SearchArgs &a, SearchSmem &sm, u
 // with the number of patterns; a word found there is compared with each
 // pattern's anchors. Marked pieces are queued per warp and verified 32 at a
 // time, one per lane, so verification work follows the number of candidates.
-// Neither the step loop nor the pattern loops are unrolled: with up to eight
-// patterns an unrolled body outgrows the instruction cache. `sink(p, piece,
+// The pattern loops are not unrolled (the step loop is): with up to eight
+// patterns a fully unrolled body outgrows the instruction cache. `sink(p, piece,
 // matches)` receives every verified piece (matches may be 0) and every
 // short-pattern piece with matches.
 template <uint32_t NP, class Sink>
@@ -224,7 +224,7 @@ __device__ __forceinline__ void filter_tile(const SearchArgs &a, SearchSmem &sm,
         else anchored |= 1u << p;
     }
     uint32_t cand = 0;  // bit 4p + k: piece k has a candidate of pattern p (patterns over 4 bytes)
-#pragma unroll 1
+#pragma unroll
     for (uint32_t k = 0; k < SR_STEPS; k++) {
         const uint32_t piece = k * SR_THREADS + tid;
         const uint4 vk = *reinterpret_cast<const uint4 *>(&sm.text[piece * 16]);
