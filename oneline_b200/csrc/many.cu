@@ -594,27 +594,11 @@ cudaError_t launch_dict_ids(const DictEmitArgs &a, cudaStream_t st) {
 
 // ----------------------------------------------------------------- emit ----
 
-// Position of the k-th (0-based) set bit of w; w has more than k set bits.
-__device__ __forceinline__ uint32_t select_bit(uint32_t w, uint32_t k) {
-    uint32_t r = 0, c;
-    c = __popc(w & 0xFFFFu);
-    if (k >= c) { k -= c; w >>= 16; r += 16; }
-    c = __popc(w & 0xFFu);
-    if (k >= c) { k -= c; w >>= 8; r += 8; }
-    c = __popc(w & 0xFu);
-    if (k >= c) { k -= c; w >>= 4; r += 4; }
-    c = __popc(w & 0x3u);
-    if (k >= c) { k -= c; w >>= 2; r += 2; }
-    c = w & 1u;
-    if (k >= c) r += 1;
-    return r;
-}
-
 // Heavy hits: block (b, h) expands words [4096b, 4096b + 4096) of bitmap h,
-// warp w the 512 words [4096b + 512w, ...), 32 words per round. A round's hits
-// are written by the whole warp to consecutive slots: lane j of each 32 finds
-// its word by a binary search over the round's word prefix sums and its bit by
-// select, so every store instruction covers 32 consecutive hits.
+// warp w the 512 words [4096b + 512w, ...), 32 words per round. Each lane
+// lists its word's hits, at their ranks from a warp scan of the popcounts, in
+// the warp's shared buffer; the warp then writes the round's hits to
+// consecutive slots, so every store instruction covers 32 consecutive hits.
 // The ids of a unique pattern and their first output slots are read once per
 // block into shared memory (up to DH_MAX_DUPS of them), not once per 32 hits.
 constexpr uint32_t DH_MAX_DUPS = 64;
@@ -623,8 +607,10 @@ __global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArg
     __shared__ uint32_t warp_tot[DH_THREADS / 32];
     __shared__ uint32_t dup_id[DH_MAX_DUPS];
     __shared__ unsigned long long dup_base[DH_MAX_DUPS];
+    __shared__ uint32_t hit_buf[DH_THREADS / 32][32 * 32];  // per warp: one round's hit offsets, in order
     const uint32_t h = blockIdx.y, b = blockIdx.x;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t *buf = hit_buf[warp];
     const uint32_t *col = a.bitmap + (size_t)h * a.n_words;
     const uint32_t u = a.heavy_u[h];
     const uint32_t d0 = a.dup_start[u], d1 = a.dup_start[u + 1];
@@ -660,20 +646,23 @@ __global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArg
             if ((int)lane >= o) inc += t;
         }
         const uint32_t excl = inc - cnt;
-        const uint32_t T = __shfl_sync(0xFFFFFFFFu, inc, 31);
+        const uint32_t T = __shfl_sync(0xFFFFFFFFu, inc, 31);  // <= 1024
+        // each lane lists its word's hit offsets at their ranks in the warp's
+        // buffer; then the warp writes them, 32 consecutive hits per store
+        {
+            uint32_t bits = word, r2 = excl;
+            const uint32_t wbase = idx * 32;
+            while (bits) {
+                const uint32_t bb = __ffs(bits) - 1;
+                bits &= bits - 1;
+                buf[r2++] = wbase + bb;
+            }
+        }
+        __syncwarp();
         for (uint32_t base = 0; base < T; base += 32) {
             const uint32_t j = base + lane;
-            // largest word i of the round with excl[i] <= j: it holds hit j
-            uint32_t i = 0;
-#pragma unroll
-            for (uint32_t step = 16; step > 0; step >>= 1) {
-                const uint32_t e = __shfl_sync(0xFFFFFFFFu, excl, i + step);
-                if (e <= j) i += step;
-            }
-            const uint32_t wi = __shfl_sync(0xFFFFFFFFu, word, i);
-            const uint32_t ei = __shfl_sync(0xFFFFFFFFu, excl, i);
             if (j < T) {
-                const uint32_t off = (w0 + r * 32 + i) * 32 + select_bit(wi, j - ei);
+                const uint32_t off = buf[j];
                 if (cached) {
                     for (uint32_t d = 0; d < n_dup; d++) {
                         const unsigned long long slot = dup_base[d] + rank + j;
@@ -688,6 +677,7 @@ __global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArg
                 }
             }
         }
+        __syncwarp();  // the buffer is refilled by the next round
         rank += T;
     }
 }
