@@ -263,7 +263,7 @@ ol_status parse_doc(ol_ctx *ctx, ol_doc *d, uint64_t est_lines, FlatNode **nodes
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "parse");
         const DocStats &hs = d->host_stats;
-        if (hs.error & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "parse: a look-back wait timed out");
+        if (hs.error & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "parse: a bounded device wait ran out");
         if (hs.error & OL_DEVERR_FIXUP) return ctx_fail(ctx, OL_ERR_CUDA, "parse: fix-up list overflow");
         if (hs.error & OL_DEVERR_CAPACITY) {
             est_lines = hs.line_count;  // exact now

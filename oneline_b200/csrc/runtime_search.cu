@@ -154,7 +154,7 @@ ol_status search_multi_host(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *
         if (e == cudaSuccess) e = cudaMemcpyAsync(tot_h, d_totals, cn * 4, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "search");
-        if (ctx->host_counters->error & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "search: a look-back wait timed out");
+        if (ctx->host_counters->error & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "search: a bounded device wait ran out");
         for (uint32_t j = 0; j < cn; j++) {
             uint32_t i = idx[c + j];
             totals[i] = tot_h[j];
