@@ -11,8 +11,16 @@ indices random bytes). Inputs (1 GiB) are larger than L2, so no flush is needed.
             tree, searches, download of offsets/kinds/tree arrays/hits);
   roofline: the dominant kernel's algorithmic bytes per launch / its average
             launch time, against the measured HBM copy bandwidth;
-  cpu_baseline: the multi-threaded C++ port of the reference's CPU engine on a
-            bounded sample of the same document.
+  cpu_baseline: the multi-threaded C++ port of the reference's CPU engine on the
+            same 1 GiB document, on all host cores, with per-stage times;
+  parity  : after the timed region, every output of the last timed step
+            (offsets, kinds, 16-byte nodes, parent, subtree_end, first_child,
+            next_sibling, every hit of the 8 patterns) compared element by
+            element with the CPU port's outputs on the same document;
+  dictionary: the 10,000-pattern dictionary search of a 1 GiB document (seed 2)
+            as a sub-record, with its own roofline, e2e, CPU baseline and
+            parity (exact per-pattern counts, an order-checking digest of all
+            hits, and the full hit lists of sampled patterns).
 
 `--impl reference` times that CPU port alone (rank 0; other ranks exit).
 Multi-GPU (torchrun): each rank parses and searches its own document (replicas,
@@ -27,6 +35,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -70,8 +79,15 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--e2e-workers", type=int, default=3, help="concurrent end-to-end steps (contexts)")
-    ap.add_argument("--cpu-sample-mb", type=int, default=256)
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-reps", type=int, default=2, help="timed CPU-port steps in the cpu_baseline leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and the parity check")
+    ap.add_argument("--no-dictionary", action="store_true",
+                    help="skip the dictionary sub-record of the default workload")
+    ap.add_argument("--dict-bytes", type=int, default=1 << 30, help="dictionary document size (default 1 GiB)")
+    ap.add_argument("--dict-cpu-sample-mb", type=int, default=128,
+                    help="prefix of the dictionary document timed on the CPU port")
+    ap.add_argument("--clock-log", default=None,
+                    help="file for the nvidia-smi clock log of the timed region (default: a temp file)")
     ap.add_argument("--no-graph", action="store_true", help="enqueue the headline step call by call, no CUDA graph")
     ap.add_argument("--profile-launches", action="store_true",
                     help="one short run for an ncu launch list (no e2e, no CPU leg)")
@@ -92,19 +108,23 @@ def parse_args():
 class ClockSampler:
     """SM clocks and clock-event (throttle) reasons sampled during the timed
     region: NVML polled every 2 ms from a thread (read-only queries), plus a
-    nvidia-smi log (100 ms) kept in gpurun_out/ for the record."""
+    nvidia-smi log (100 ms) written to `log_path` (default: a temp file)."""
 
     REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
                ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
                ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
                ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
+    log_path = None  # set from --clock-log
+
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.samples = []
         self.max_mhz = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        base = ClockSampler.log_path or os.path.join(tempfile.gettempdir(), "oneline_clocks.csv")
+        root, ext = os.path.splitext(base)
+        self.path = f"{root}_rank{index}{ext or '.csv'}"
 
     def _poll(self):
         import pynvml
@@ -120,7 +140,7 @@ class ClockSampler:
     def __enter__(self):
         import threading
 
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        os.makedirs(os.path.dirname(self.path) or ".", exist_ok=True)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -241,63 +261,140 @@ def make_workload(nbytes: int, seed: int, pattern_source_bytes: int = 0):
     return text, pats
 
 
-def cpu_leg(text: np.ndarray, pats, sample_mb: int, reps: int = 2) -> dict:
-    """The reference CPU path (port) on all host cores over a bounded prefix."""
-    import oracle
+class CpuPort:
+    """The reference's CPU path on one document: the multi-threaded C++ port of
+    oneline-simd (parse_par, build_links + first_child/next_sibling, one
+    find_all_par per pattern) on `threads` host cores. Outputs are allocated
+    once and reused by every step, as ParseBuffers does
+    (crates/oneline-simd/src/lib.rs:445-469); each search writes into a buffer
+    sized by a first run. The outputs of the last step are the parity reference
+    for the GPU's."""
 
-    n = min(text.size, sample_mb << 20)
-    sample = text[:n]
-    # cut at a line boundary so the sample is a document of its own
-    cut = int(np.nonzero(sample == 10)[0][-1]) + 1
-    sample = np.ascontiguousarray(sample[:cut])
-    base = oracle.CpuBaseline()
-    times = []
-    for _ in range(reps + 1):
+    STAGES = ("parse_par", "build_links", "find_all_par")
+
+    def __init__(self, text: np.ndarray, pats, threads: int | None = None):
+        import oracle
+
+        self.base = oracle.CpuBaseline(threads)
+        self.threads = self.base.threads
+        self.text = np.ascontiguousarray(text)
+        self.pats = [bytes(x) for x in pats]
+        n = self.base.line_count(self.text)
+        self.lines = n
+        self.offsets = np.empty(max(n, 1), np.uint32)
+        self.nodes = np.empty(max(n, 1), oracle.NODE_DTYPE)
+        self.tree = {k: np.empty(max(n, 1), np.uint32) for k in TREE_KEYS}
+        self.totals = [self.base.find_all_par(self.text, x, np.empty(1, np.uint32))[0] for x in self.pats]
+        self.hits = [np.empty(max(t, 1), np.uint32) for t in self.totals]
+
+    def step(self) -> dict:
+        """One pass of the path; returns the seconds per stage."""
         t0 = time.perf_counter()
-        offs, nodes = base.parse_par(sample)
-        base.build_links(nodes)
-        for p in pats:
-            base.find_all_par(sample, p)
-        times.append(time.perf_counter() - t0)
-    t = statistics.median(times[1:])
-    return {"value": round(sample.size / t / 1e9, 4), "unit": "GB/s", "cores": base.threads, "kind": "port",
-            "sample": f"first {sample.size} bytes of the same document (line-aligned): parse_par + build_links + "
-                      f"children + {len(pats)} x find_all_par, median of {reps} after 1 warm-up "
-                      "(C++ port of oneline-simd; the Rust reference cannot be built here)",
-            "seconds_per_rep": round(t, 4)}
+        got = self.base.parse_par_into(self.text.ctypes.data, self.text.size, self.offsets, self.nodes)
+        assert got == self.lines
+        t1 = time.perf_counter()
+        self.base.build_links(self.nodes[: self.lines], out=self.tree)
+        t2 = time.perf_counter()
+        for i, x in enumerate(self.pats):
+            total, _ = self.base.find_all_par(self.text, x, self.hits[i])
+            assert total == self.totals[i]
+        t3 = time.perf_counter()
+        return {"parse_par": t1 - t0, "build_links": t2 - t1, "find_all_par": t3 - t2, "step": t3 - t0}
+
+
+TREE_KEYS = ("parent", "subtree_end", "first_child", "next_sibling")
+
+# The reference's published CPU figures for these stages (RTX 3060 host, 12
+# threads; .agents/tasks/*.md), scaled per thread for comparison.
+PUBLISHED_CPU = {
+    "parse_par": {"value": "1 GiB HTML in 64 ms (16.8 GB/s) on 12 threads",
+                  "source": ".agents/tasks/gpu-profiling-and-overhead.md:139"},
+    "build_links": {"value": "1 GiB mixed (13 M lines) in 40.2 ms on 12 threads",
+                    "source": ".agents/tasks/gpu-tree-construction.md:14"},
+    "find_all_par": {"value": "1 GiB, one sparse pattern, 27 ms on 12 threads",
+                     "source": ".agents/tasks/gpu-substring-search.md:151"},
+}
+
+
+def cpu_leg(text: np.ndarray, pats, reps: int = 2) -> tuple[dict, CpuPort]:
+    """The reference CPU path (port) on all host cores over the whole document:
+    one warm-up step, then the median of `reps` steps, with per-stage times."""
+    port = CpuPort(text, pats)
+    port.step()
+    runs = [port.step() for _ in range(max(reps, 1))]
+    med = {k: statistics.median(r[k] for r in runs) for k in runs[0]}
+    n = port.text.size
+    stages = {k: {"ms": round(med[k] * 1e3, 2), "published": PUBLISHED_CPU[k]} for k in CpuPort.STAGES}
+    stages["parse_par"]["gb_per_s"] = round(n / med["parse_par"] / 1e9, 3)
+    stages["build_links"]["ns_per_line_thread"] = round(med["build_links"] * 1e9 * port.threads / max(port.lines, 1), 1)
+    stages["find_all_par"]["patterns"] = len(port.pats)
+    rec = {"value": round(n / med["step"] / 1e9, 4), "unit": "GB/s", "cores": port.threads, "kind": "port",
+           "sample": f"the whole {n}-byte document (the same config as the GPU line): parse_par + build_links + "
+                     f"children + {len(port.pats)} x find_all_par into preallocated outputs, median of {len(runs)} "
+                     "after 1 warm-up (C++ port of oneline-simd; the Rust reference cannot be built here)",
+           "seconds_per_rep": round(med["step"], 4), "stages": stages}
+    return rec, port
+
+
+def first_mismatch(name: str, got: np.ndarray, want: np.ndarray):
+    """None when equal, else a one-line description of the first difference."""
+    got, want = np.asarray(got), np.asarray(want)
+    if got.shape != want.shape:
+        return f"{name}: {got.size} entries vs {want.size}"
+    bad = np.flatnonzero(got != want)
+    if bad.size == 0:
+        return None
+    i = int(bad[0])
+    return f"{name}[{i}]: {got[i]} vs {want[i]} ({bad.size} differ)"
+
+
+def parity_parse_search(doc, tree, parser, hit_outs, d_totals, port: CpuPort) -> dict:
+    """Every output of the GPU's last step against the CPU port on the same
+    document, element by element (the port is itself checked against the oracle
+    in the CPU tests)."""
+    L = port.lines
+    checks = []
+    got_offs = doc.read_offsets()
+    checks.append(first_mismatch("offsets", got_offs, port.offsets[:L]))
+    checks.append(first_mismatch("kinds", doc.read_kinds(), port.nodes["kind"][:L].astype(np.uint8)))
+    nodes = doc.read_nodes()
+    for f in ("depth", "kind", "span_start", "span_len"):
+        checks.append(first_mismatch(f"nodes.{f}", nodes[f], port.nodes[f][:L]))
+    t = parser.download_tree(tree)
+    for k in TREE_KEYS:
+        checks.append(first_mismatch(k, t[k], port.tree[k][:L]))
+    tots = d_totals.cpu().numpy().view(np.uint32)
+    for i, (o, want_t) in enumerate(zip(hit_outs, port.totals)):
+        checks.append(None if int(tots[i]) == want_t else f"total[{i}]: {int(tots[i])} vs {want_t}")
+        checks.append(first_mismatch(f"hits[{i}]", o[:want_t].cpu().numpy().view(np.uint32), port.hits[i][:want_t]))
+    bad = [c for c in checks if c]
+    return {"result": "bit-exact" if not bad else "MISMATCH", "first_mismatch": bad[0] if bad else None,
+            "compared": f"{L} offsets, kinds and 16-byte nodes; parent, subtree_end, first_child, next_sibling; "
+                        f"{sum(port.totals)} hits of {len(port.totals)} patterns",
+            "against": f"the CPU port of oneline-simd on the same document ({port.threads} threads)"}
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
     text, pats = make_workload(args.bytes, args.seed)
-    import oracle
-
-    n = min(text.size, args.cpu_sample_mb << 20)
-    cut = int(np.nonzero(text[:n] == 10)[0][-1]) + 1
-    sample = np.ascontiguousarray(text[:cut])
-    base = oracle.CpuBaseline()
-
-    def step():
-        offs, nodes = base.parse_par(sample)
-        base.build_links(nodes)
-        for p in pats:
-            base.find_all_par(sample, p)
-
+    port = CpuPort(text, pats)
     for _ in range(args.warmup):
-        step()
+        port.step()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step()
+    runs = [port.step() for _ in range(args.steps)]
     dt = (time.perf_counter() - t0) / args.steps
-    v = sample.size / dt / 1e9
+    v = text.size / dt / 1e9
+    med = {k: round(statistics.median(r[k] for r in runs) * 1e3, 2) for k in CpuPort.STAGES}
     line = {"metric": METRIC, "value": round(v, 4), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": workload_config(args, sample.size, pats, None),
-            "cpu_baseline": {"value": round(v, 4), "unit": "GB/s", "cores": base.threads, "kind": "port",
-                             "sample": f"first {sample.size} bytes of the {args.bytes}-byte document per step "
-                                       "(C++ port of oneline-simd on all host threads)"},
+            "config": workload_config(args, text.size, pats, port.lines),
+            "cpu_baseline": {"value": round(v, 4), "unit": "GB/s", "cores": port.threads, "kind": "port",
+                             "sample": f"the whole {text.size}-byte document every step: parse_par + build_links + "
+                                       f"children + {len(pats)} x find_all_par into preallocated outputs (C++ port "
+                                       "of oneline-simd on all host threads)",
+                             "stage_ms": med},
             "e2e": {"value": round(v, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -510,39 +607,139 @@ def run_ours(args, world, rank, local):
                        "ol_doc_read_offsets/kinds + ol_tree_read (4 arrays), on `workers` contexts at once, "
                        "one upload and one download in flight at a time"}
 
-    cpu = None
-    if rank == 0 and not args.no_cpu:
-        cpu = cpu_leg(text, pats, args.cpu_sample_mb)
+    # CPU baseline (rank 0, all host cores, while the other ranks wait), then
+    # parity on every rank: the outputs of the last timed step against the CPU
+    # port on the same document (rank 0 reuses its timed port's outputs).
+    cpu, parity = None, None
+    if not args.no_cpu:
+        port = None
+        if rank == 0:
+            cpu, port = cpu_leg(text, pats, args.cpu_reps)
+        barrier(world)
+        if port is None:
+            port = CpuPort(text, pats, threads=max(1, (os.cpu_count() or 1) // world))
+            port.step()
+        parity = parity_parse_search(doc, tree, p, outs, d_tot, port)
+        bad = allreduce_sum(0.0 if parity["result"] == "bit-exact" else 1.0, world)
+        if world > 1:
+            parity["ranks_checked"] = world
+            parity["ranks_mismatched"] = int(bad)
+        del port
+
+    dict_rec = None
+    if not args.no_dictionary:
+        if not args.no_graph:
+            pipe.free()
+        del outs
+        dict_rec = dictionary_record(args, world, rank, local, p)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u8", "data": "synthetic",
                 "config": {**workload_config(args, N, pats, lines), "hits": totals},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "e2e": e2e,
                 "gpu_launches": int(launches), "clocks": clocks.summary(),
                 "step_form": "CUDA graph (ol_pipeline_launch)" if not args.no_graph else "enqueued calls",
-                "device": p.adapter_name()}
+                "dictionary": dict_rec, "device": p.adapter_name()}
         print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------ dictionary
 
-def run_dictionary(args, world, rank, local):
-    """1 GiB synthetic document (seed 2) against 10,000 patterns of 4..64 B: every
-    (pattern id, offset) hit in (pattern, offset) order, left in HBM (value) or
-    downloaded (e2e)."""
+_U64 = (1 << 64) - 1
+
+
+def _i64(c: int) -> int:
+    """A 64-bit constant as torch's signed int64."""
+    return c - (1 << 64) if c >= 1 << 63 else c
+
+
+def device_hit_digest(hits_i32, total: int, chunk: int = 1 << 27) -> int:
+    """The order-checking digest of a device hit list {pattern u32, offset u32}[total]:
+    the sum over slots i of the CPU port's hit_digest(i, pattern, offset) mod 2^64,
+    computed with torch on the device in chunks (int64 arithmetic wraps)."""
+    import torch
+
+    def lsr(x, k):  # logical shift right of int64
+        return (x >> k) & ((1 << (64 - k)) - 1)
+
+    v64 = hits_i32.view(torch.int64)[:total]
+    k0, k1, k2 = _i64(0x9E3779B97F4A7C15), _i64(0xBF58476D1CE4E5B9), _i64(0x94D049BB133111EB)
+    acc = 0
+    for s0 in range(0, total, chunk):
+        v = v64[s0: s0 + chunk]
+        slot = torch.arange(s0, s0 + v.numel(), dtype=torch.int64, device=v.device)
+        x = ((v << 32) | lsr(v, 32)) ^ (slot * k0)  # (pattern << 32) | offset
+        del slot
+        x = x ^ lsr(x, 30)
+        x = x * k1
+        x = x ^ lsr(x, 27)
+        x = x * k2
+        x = x ^ lsr(x, 31)
+        acc += int(x.sum().item())
+        del x
+    return acc & _U64
+
+
+def parity_dictionary(text: np.ndarray, pats, counts: np.ndarray, total: int, d_hits, threads: int) -> dict:
+    """The GPU's dictionary result over the whole document against the CPU port:
+    every pattern's count, the total and the order-checking digest of all hits
+    (hit_digest summed over the (pattern, offset)-ordered slots, without
+    building the list on the host), plus, element by element, the full hit lists
+    of the three most frequent patterns and five others (find_all_par on the
+    whole document)."""
+    import oracle
+
+    base = oracle.CpuBaseline(threads)
+    many = base.many(pats)
+    t0 = time.perf_counter()
+    want_counts, want_total, want_digest = many.digest_par(text)
+    t_digest = time.perf_counter() - t0
+    checks = [first_mismatch("counts", counts.astype(np.uint64), want_counts),
+              None if total == want_total else f"total: {total} vs {want_total}"]
+    got_digest = device_hit_digest(d_hits, total)
+    checks.append(None if got_digest == want_digest else f"digest: {got_digest:#x} vs {want_digest:#x}")
+    base_of = np.concatenate([[0], np.cumsum(want_counts.astype(np.int64))])
+    order = np.argsort(-want_counts.astype(np.int64), kind="stable")
+    rng = np.random.default_rng(7)
+    sampled = [int(i) for i in order[:3]] + [int(i) for i in rng.choice(len(pats), 5, replace=False)]
+    listed = 0
+    for i in sampled:
+        c = int(want_counts[i])
+        want = np.empty(max(c, 1), np.uint32)
+        n_found, _ = base.find_all_par(text, pats[i], want)
+        got = d_hits[2 * int(base_of[i]): 2 * (int(base_of[i]) + c)].cpu().numpy().view(np.uint32).reshape(-1, 2)
+        checks.append(None if n_found == c else f"pattern {i}: find_all_par {n_found} vs count {c}")
+        checks.append(first_mismatch(f"hits of pattern {i} (pattern field)", got[:, 0], np.full(c, i, np.uint32)))
+        checks.append(first_mismatch(f"hits of pattern {i} (offsets)", got[:, 1], want[:c]))
+        listed += c
+    bad = [c for c in checks if c]
+    return {"result": "bit-exact" if not bad else "MISMATCH", "first_mismatch": bad[0] if bad else None,
+            "compared": f"counts of all {len(pats)} patterns, the total ({total} hits) and a 64-bit order-checking "
+                        f"digest of every (pattern, offset) hit in order; {listed} hits of {len(sampled)} patterns "
+                        "element by element",
+            "against": f"the CPU port's Aho-Corasick DFA ({many.states} states) and find_all_par on the same "
+                       f"document ({threads} threads)",
+            "cpu_check_s": round(t_digest, 2)}
+
+
+def dictionary_record(args, world, rank, local, p=None) -> dict:
+    """A synthetic oneline document (seed 2, 1 GiB) against 10,000 patterns of
+    4..64 B: every (pattern id, offset) hit in (pattern, offset) order, left in
+    HBM (value) or downloaded (e2e). Returns the record (all ranks take part in
+    the collectives; the record is meaningful on rank 0)."""
     import torch
 
     from oneline_b200 import GpuParser, _lib, datagen
 
     L = _lib.load()
     seed = 2 + rank
-    text = datagen.corpus(args.bytes, seed)
+    text = datagen.corpus(args.dict_bytes, seed)
     pats = datagen.patterns_dictionary(text, seed, n=10_000)
     N = text.size
     torch.cuda.set_device(local)
-    p = GpuParser(local)
+    p = p or GpuParser(local)
     host = torch.empty(N, dtype=torch.uint8, pin_memory=True)
     host.numpy()[:] = text
     doc = p.upload(host.numpy())
@@ -554,12 +751,13 @@ def run_dictionary(args, world, rank, local):
     def step():
         c, t = p.search_many_device(doc, ps, hits.data_ptr(), total)
         assert t == total
+        return c
 
     if args.profile_launches:
         for _ in range(args.warmup + args.steps):
             step()
         p.sync()
-        return
+        return {}
     for _ in range(args.warmup):
         step()
     p.sync()
@@ -571,7 +769,7 @@ def run_dictionary(args, world, rank, local):
         with torch.cuda.stream(stream):
             ev0.record()
         for _ in range(args.steps):
-            step()
+            counts = step()
         with torch.cuda.stream(stream):
             ev1.record()
         ev1.synchronize()
@@ -584,6 +782,10 @@ def run_dictionary(args, world, rank, local):
     alg = N + 8 * total  # text once + every ManyHit {pattern u32, offset u32} once
     achieved = alg / (ms * 1e-3) / 1e9
 
+    def chk(s):
+        if s != 0:
+            raise RuntimeError(L.ol_last_error(p.ctx).decode())
+
     e2e = None
     if args.e2e_steps > 0:
         out_h = torch.empty(2 * max(total, 1), dtype=torch.int32, pin_memory=True)
@@ -592,7 +794,6 @@ def run_dictionary(args, world, rank, local):
 
         def e2e_step():
             h = ctypes.c_void_p()
-            chk = lambda s: (_ for _ in ()).throw(RuntimeError(L.ol_last_error(p.ctx).decode())) if s else None  # noqa
             chk(L.ol_doc_upload(p.ctx, host.data_ptr(), N, ctypes.byref(h)))
             chk(L.ol_search_many(p.ctx, h.value, ps.handle, total, cnt_h.ctypes.data, ctypes.byref(tot_h),
                                  out_h.data_ptr()))
@@ -603,50 +804,65 @@ def run_dictionary(args, world, rank, local):
         for _ in range(args.e2e_steps):
             e2e_step()
         dt = allreduce_max((time.perf_counter() - t0) / args.e2e_steps, world)
+        assert int(tot_h.value) == total
+        del out_h
         e2e = {"value": round(bytes_all / dt / 1e9, 4), "unit": "GB/s", "ms_per_step": round(dt * 1e3, 2),
                "h2d_bytes_per_step": int(N), "d2h_bytes_per_step": int(8 * total + 4 * len(pats) + 8),
                "timing": "host wall clock around blocking C-ABI calls, max over ranks",
                "path": "ol_doc_upload (pinned text) + ol_search_many (counts and every hit to pinned host memory)"}
 
-    cpu = None
-    if rank == 0 and not args.no_cpu:
+    cpu, parity = None, None
+    if not args.no_cpu:
         import oracle
 
-        n = min(N, 32 << 20)
-        sample = np.ascontiguousarray(text[:n])
-        many = oracle.CpuBaseline().many(pats)
-        ts = []
-        for _ in range(3):
-            t0 = time.perf_counter()
-            many.find_all_par(sample)
-            ts.append(time.perf_counter() - t0)
-        t = statistics.median(ts[1:])
-        cpu = {"value": round(n / t / 1e9, 4), "unit": "GB/s", "cores": many.threads, "kind": "port",
-               "sample": f"first {n} bytes of the same document x the same 10,000 patterns: Aho-Corasick DFA "
-                         f"(byte classes), all hits sorted by (pattern, offset); median of 2 after 1 warm-up",
-               "dfa_states": int(many.states)}
+        if rank == 0:
+            n = min(N, args.dict_cpu_sample_mb << 20)
+            sample = np.ascontiguousarray(text[:n])
+            many = oracle.CpuBaseline().many(pats)
+            ts = []
+            for _ in range(2):
+                t0 = time.perf_counter()
+                many.find_all_par(sample)
+                ts.append(time.perf_counter() - t0)
+            t = ts[-1]
+            cpu = {"value": round(n / t / 1e9, 4), "unit": "GB/s", "cores": many.threads, "kind": "port",
+                   "sample": f"first {n} bytes of the same document x the same 10,000 patterns: Aho-Corasick DFA "
+                             "(byte classes), every hit, ordered by (pattern, offset); the second of 2 runs (the "
+                             "whole 1 GiB would hold 30 GB of hits in host memory)",
+                   "dfa_states": int(many.states)}
+            del many
+        barrier(world)
+        parity = parity_dictionary(text, pats, counts, total, hits, max(1, (os.cpu_count() or 1) // world))
+        bad = allreduce_sum(0.0 if parity["result"] == "bit-exact" else 1.0, world)
+        if world > 1:
+            parity["ranks_checked"] = world
+            parity["ranks_mismatched"] = int(bad)
 
-    if rank == 0:
-        line = {"metric": "dictionary search GB/s vs HBM peak", "value": round(value, 3), "unit": "GB/s",
-                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-                "data": "synthetic",
-                "config": {"workload": f"{N}-byte synthetic oneline document (seed {seed}) x 10,000-pattern "
-                                       f"dictionary (4..64 B, 60% sampled from the text): every (pattern, offset)",
-                           "text_bytes": int(N), "patterns": len(pats), "unique_patterns": ps.unique(),
-                           "total_hits": int(total), "hit_bytes": int(8 * total),
-                           "walked_per_byte": round(work["walked"] / N, 4),
-                           "nodes_per_walk": round(work["nodes"] / max(work["walked"], 1), 2),
-                           "bitmap_patterns": work["heavy_patterns"], "sorted_key_hits": work["light_hits"],
-                           "l2": "inputs and outputs larger than L2 (no flush needed)",
-                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-                "roofline": {"bound": "hbm", "kernel": "dictionary pass (match, rank, sort, emit)",
-                             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                             "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
-                             "alg_bytes_per_launch": int(alg), "ms_per_launch": round(ms, 3)},
-                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks.summary(),
-                "device": p.adapter_name()}
-        print(json.dumps(line), flush=True)
+    return {"metric": "dictionary search GB/s vs HBM peak", "value": round(value, 3), "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic",
+            "config": {"workload": f"{N}-byte synthetic oneline document (seed {seed}) x 10,000-pattern "
+                                   f"dictionary (4..64 B, 60% sampled from the text): every (pattern, offset)",
+                       "text_bytes": int(N), "patterns": len(pats), "unique_patterns": ps.unique(),
+                       "total_hits": int(total), "hit_bytes": int(8 * total),
+                       "walked_per_byte": round(work["walked"] / N, 4),
+                       "nodes_per_walk": round(work["nodes"] / max(work["walked"], 1), 2),
+                       "bitmap_patterns": work["heavy_patterns"], "sorted_key_hits": work["light_hits"],
+                       "l2": "inputs and outputs larger than L2 (no flush needed)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "kernel": "dictionary pass (match, rank, sort, emit)",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
+                         "alg_bytes_per_launch": int(alg), "ms_per_launch": round(ms, 3)},
+            "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clocks.summary(), "device": p.adapter_name()}
+
+
+def run_dictionary(args, world, rank, local):
+    rec = dictionary_record(args, world, rank, local)
+    if rank == 0 and rec:
+        print(json.dumps(rec), flush=True)
 
 
 # ----------------------------------------------------------------- batch
@@ -893,6 +1109,7 @@ def run_serve(args, world, rank, local):
 
 def main():
     args = parse_args()
+    ClockSampler.log_path = args.clock_log
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":

@@ -82,6 +82,15 @@ ol_status ol_ctx_device_name(ol_ctx *ctx, char *buf, size_t cap);
 ol_status ol_ctx_sync(ol_ctx *ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order work. */
 void *ol_ctx_stream(ol_ctx *ctx);
+/* Test hook, like the reference's test-only candidate_capacity_cap
+ * (crates/oneline-gpu/src/parser.rs:20-23, many.rs:450-458): arms host-side
+ * faults for the next operation on ctx that they name, so that error paths run
+ * without faulting the GPU. OL_INJECT_DICT_WAIT_TIMEOUT: the next dictionary
+ * search's blocks take their bounded-wait timeout branch once their filter
+ * copy has landed; the call returns OL_ERR_TIMEOUT and the context stays
+ * usable. 0 disarms. */
+#define OL_INJECT_DICT_WAIT_TIMEOUT 1u
+ol_status ol_ctx_inject(ol_ctx *ctx, uint32_t faults);
 /* Kernels this library has launched in this process, over all contexts (every
  * launch counts itself). For benchmarks; no reference counterpart. */
 uint64_t ol_launch_count(void);
@@ -328,7 +337,9 @@ ol_status ol_server_stats(ol_server *server, uint64_t *resident_docs, uint64_t *
  *   text_cap    bytes readable at d_text, at least OL_NOALLOC_TEXT_CAP(text_len)
  *               (whole 16 KiB tiles plus 64 bytes; what lies past text_len is
  *               read but never matched, so it may hold anything).
- *   pattern     host memory, 1..OL_MAX_PATTERN_LEN bytes, copied before return.
+ *   pattern     host memory, 1..OL_MAX_PATTERN_LEN bytes, read before return
+ *               (its bytes travel in a kernel's arguments): the buffer may be
+ *               overwritten as soon as the call returns, pinned or not.
  *   d_total     device u32: the number of occurrences.
  *   d_out       device u32[max_matches]: the first min(total, max_matches)
  *               offsets, ascending (may be NULL when max_matches is 0).
@@ -337,8 +348,9 @@ ol_status ol_server_stats(ol_server *server, uint64_t *resident_docs, uint64_t *
  *   err/err_cap optional buffer for a message when the status is not OL_OK.
  *
  * Call it with the device that owns the buffers current. The first call on a
- * device looks up the scratch array's device address (cudaGetSymbolAddress);
- * make that first call before any stream capture. Every call on a device uses
+ * device looks up the scratch array's device address (cudaGetSymbolAddress),
+ * and so does the first call after the device's context was created anew
+ * (cudaDeviceReset); make that first call before any stream capture. Every call on a device uses
  * the same scratch array: calls that overlap on the GPU (on streams with no
  * ordering between them) race and may return wrong results. */
 #define OL_NOALLOC_MAX_TEXT_LEN (256ull << 20)

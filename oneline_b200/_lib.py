@@ -35,6 +35,7 @@ SIGNATURES: dict[str, tuple] = {
     "ol_ctx_device_name": (_S, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     "ol_ctx_sync": (_S, [_P]),
     "ol_ctx_stream": (_P, [_P]),
+    "ol_ctx_inject": (_S, [_P, _U32]),
     "ol_launch_count": (_U64, []),
     "ol_doc_upload": (_S, [_P, _U8P, _U64, _PP]),
     "ol_doc_upload_device": (_S, [_P, _U8P, _U64, _PP]),

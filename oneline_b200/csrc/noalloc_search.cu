@@ -10,11 +10,16 @@
 // fixed array below that every GPU which loads this library holds until the
 // process exits.
 //
+// The pattern reaches the device inside the arguments of a one-block kernel
+// that writes it into the array, so the call reads the caller's pattern
+// buffer only while it runs: the caller may overwrite that buffer (pageable or
+// pinned) as soon as the call returns.
+//
 // The array is shared by every call on a device and keeps what the last call
 // left in it. Nothing a call reads from it is left over from an earlier call:
-// the pattern is copied in, the count launch writes every tile's count and the
-// scan writes every base and the total, before anything reads them. Two calls
-// whose work overlaps on the GPU (different streams, no ordering between
+// the pattern is written in, the count launch writes every tile's count and
+// the scan writes every base and the total, before anything reads them. Two
+// calls whose work overlaps on the GPU (different streams, no ordering between
 // them) race on the array and may both return wrong results.
 #include <cuda_runtime.h>
 
@@ -38,11 +43,31 @@ static_assert(((OL_MAX_PATTERN_LEN - 1 + 15) & ~15u) <= ol::kSearchMaxStagedPatt
 
 // Device scratch. Host code must not pass this name to a kernel: on the host
 // it is only a stand-in for the symbol. Its device address comes from
-// cudaGetSymbolAddress, once per device.
+// cudaGetSymbolAddress, once per device (and again if the device's context is
+// ever created anew).
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kScratchBytes];
 
+// The pattern bytes, passed by value as a kernel argument.
+struct PatternBytes {
+    uint8_t b[OL_MAX_PATTERN_LEN];
+};
+
+__global__ void noalloc_put_pattern_kernel(PatternBytes p, uint32_t len, uint8_t *dst) {
+    if (threadIdx.x < len) dst[threadIdx.x] = p.b[threadIdx.x];
+}
+
+// The scratch array's device address per device, with the CUDA context it was
+// looked up in: a device whose primary context was destroyed and created again
+// (cudaDeviceReset) gets a new set-up instead of a stale address.
+struct ScratchSetup {
+    void *context = nullptr;
+    uint8_t *ptr = nullptr;
+};
 std::mutex g_setup_mu;
-uint8_t *g_scratch_ptr[kMaxDevices] = {};
+ScratchSetup g_setup[kMaxDevices];
+
+typedef int (*CtxGetCurrentFn)(void **);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
 
 ol_status fail(char *err, uint32_t err_cap, ol_status s, const char *fmt, unsigned long long a = 0,
                unsigned long long b = 0) {
@@ -90,16 +115,33 @@ extern "C" ol_status ol_search_noalloc(const uint8_t *d_text, uint64_t text_len,
     uint8_t *scratch;
     {
         std::lock_guard<std::mutex> g(g_setup_mu);
-        if (!g_scratch_ptr[dev]) {
+        if (!g_ctx_get_current) {
+            void *fn = nullptr;
+            cudaDriverEntryPointQueryResult q;
+            e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+            if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+                return fail(err, err_cap, OL_ERR_CUDA,
+                            "ol_search_noalloc: the driver's cuCtxGetCurrent is unavailable (error %llu)", (unsigned)e);
+            g_ctx_get_current = (CtxGetCurrentFn)fn;
+        }
+        // cudaSetDevice makes the device's primary context current (CUDA 12+)
+        e = cudaSetDevice(dev);
+        void *cur = nullptr;
+        if (e != cudaSuccess || g_ctx_get_current(&cur) != 0 || !cur)
+            return fail(err, err_cap, OL_ERR_CUDA, "ol_search_noalloc: no current CUDA context (error %llu)",
+                        (unsigned)e);
+        ScratchSetup &su = g_setup[dev];
+        if (!su.ptr || su.context != cur) {
             uint8_t *p = nullptr;
             e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
             if (e != cudaSuccess || !p)
                 return fail(err, err_cap, OL_ERR_CUDA,
                             "ol_search_noalloc: cudaGetSymbolAddress of the scratch array failed (error %llu)",
                             (unsigned)e);
-            g_scratch_ptr[dev] = p;
+            su.context = cur;
+            su.ptr = p;
         }
-        scratch = g_scratch_ptr[dev];
+        scratch = su.ptr;
     }
 
     cudaStream_t st = (cudaStream_t)stream;
@@ -110,11 +152,15 @@ extern "C" ol_status ol_search_noalloc(const uint8_t *d_text, uint64_t text_len,
                                 : fail(err, err_cap, OL_ERR_CUDA, "ol_search_noalloc: cudaMemsetAsync failed (error %llu)",
                                        (unsigned)e);
     }
-    // The pattern is copied from the caller's host memory into the array; the
-    // caller may reuse its pattern buffer as soon as this call returns.
-    e = cudaMemcpyAsync(scratch, pattern, pat_len, cudaMemcpyHostToDevice, st);
+    // The pattern goes into the array through a kernel argument: its bytes are
+    // taken from the caller's buffer here, before this call returns.
+    PatternBytes pb{};
+    memcpy(pb.b, pattern, pat_len);
+    noalloc_put_pattern_kernel<<<1, OL_MAX_PATTERN_LEN, 0, st>>>(pb, pat_len, scratch);
+    OL_LAUNCHED();
+    e = cudaGetLastError();
     if (e != cudaSuccess)
-        return fail(err, err_cap, OL_ERR_CUDA, "ol_search_noalloc: pattern copy failed (error %llu)", (unsigned)e);
+        return fail(err, err_cap, OL_ERR_CUDA, "ol_search_noalloc: pattern write failed (error %llu)", (unsigned)e);
 
     ol::SearchArgs a{};
     a.text = d_text;

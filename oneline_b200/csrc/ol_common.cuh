@@ -1,11 +1,10 @@
 // Device-side building blocks shared by the oneline sm_100a kernels.
 //
 // * NodeKind codes and FlatNode layout (crates/oneline-core/src/lib.rs:39-96).
-// * Decoupled look-back primitives: every tile publishes a 64-bit word
-//   [status:2 | value:32] per value it carries, readers poll with bounded spins.
-// * Device status words: a kernel never traps or spins forever; a wait that runs
-//   past its limit sets OL_DEVERR_TIMEOUT and the kernel finishes with garbage
-//   that the host discards after reading the status.
+// * Device status words: a kernel never traps or spins forever; the one
+//   bounded wait (the dictionary kernel's bulk-copy barrier) sets
+//   OL_DEVERR_TIMEOUT when it runs out and the host discards the results.
+// * Byte SWAR helpers and the line classifier.
 #pragma once
 #include <cstdint>
 
@@ -36,34 +35,14 @@ constexpr uint32_t OL_DEVERR_DEEP = 1u << 3;      // a content line deeper than 
 
 // Per-launch counters that live in device memory next to a document.
 struct DocStats {
-    uint32_t ticket;            // dynamic tile counter of the parse kernel
     uint32_t line_count;        // lines in the document
     uint32_t max_content_depth; // deepest non-blank line (saturates at 0xFFFFFFFF)
     uint32_t fixup_count;       // lines classified by the fix-up kernel
     uint32_t error;             // OL_DEVERR_* bits
-    uint32_t tree_ticket_fwd;   // dynamic tile counters of the tree kernels
-    uint32_t tree_ticket_bwd;
-    uint32_t search_ticket;
-    uint32_t pad[8];
+    uint32_t pad[12];
 };
 
 // ---------------------------------------------------------- memory access --
-
-__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t *p) {
-    uint64_t v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_relaxed_u64(uint64_t *p, uint64_t v) {
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
-    uint32_t v;
-    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 
 // Streaming 16-byte load (read once: do not keep in L1).
 __device__ __forceinline__ uint4 ld_stream16(const void *p) {
@@ -72,136 +51,6 @@ __device__ __forceinline__ uint4 ld_stream16(const void *p) {
                  : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
                  : "l"(p));
     return v;
-}
-
-__device__ __forceinline__ uint64_t globaltimer_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// ------------------------------------------------------------ look-back ----
-
-constexpr uint64_t LB_AGGREGATE = 1ull << 32;
-constexpr uint64_t LB_PREFIX = 2ull << 32;
-constexpr uint64_t LB_STATUS_MASK = 3ull << 32;
-// A wait gives up after this long (ns) or this many polls, whichever first.
-constexpr uint64_t LB_WAIT_NS = 1000000000ull;  // 1 s
-constexpr uint32_t LB_WAIT_POLLS = 1u << 26;
-
-// Waits until word `p` has a non-zero status; returns it. On timeout (or when
-// another block already reported an error) sets OL_DEVERR_TIMEOUT in *err and
-// returns a PREFIX word with value 0 so that the caller stops walking.
-__device__ __forceinline__ uint64_t lb_wait(const uint64_t *p, uint32_t *err) {
-    uint64_t w = ld_relaxed_u64(p);
-    if (w & LB_STATUS_MASK) return w;
-    uint64_t t0 = globaltimer_ns();
-    uint32_t ns = 32;
-    for (uint32_t polls = 0;; polls++) {
-        w = ld_relaxed_u64(p);
-        if (w & LB_STATUS_MASK) return w;
-        if ((polls & 63) == 63) {
-            if (ld_relaxed_u32(err) != 0 || globaltimer_ns() - t0 > LB_WAIT_NS || polls > LB_WAIT_POLLS) {
-                atomicOr(err, OL_DEVERR_TIMEOUT);
-                return LB_PREFIX;
-            }
-        }
-        __nanosleep(ns);
-        if (ns < 1024) ns <<= 1;
-    }
-}
-
-// Sum look-back over tiles 0..tile-1 done by one full warp (32-tile windows).
-// Tile t's word is status[t * stride]. Returns the exclusive prefix of `tile`;
-// all lanes get it.
-__device__ __forceinline__ uint32_t lb_sum_exclusive(const uint64_t *status, uint32_t tile, uint32_t *err,
-                                                     uint32_t stride = 1) {
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t acc = 0;
-    int64_t end = (int64_t)tile;  // window is [end-32, end)
-    while (end > 0) {
-        int64_t idx = end - 32 + (int64_t)lane;
-        uint64_t w = idx >= 0 ? lb_wait(status + idx * stride, err) : LB_PREFIX;  // before tile 0: prefix 0
-        uint32_t is_prefix = __ballot_sync(0xFFFFFFFFu, (w & LB_STATUS_MASK) == LB_PREFIX);
-        uint32_t v = (uint32_t)w;
-        if (is_prefix) {
-            int hi = 31 - __clz(is_prefix);  // nearest prefix in the window
-            uint32_t take = (int)lane >= hi ? v : 0;
-            for (int o = 16; o > 0; o >>= 1) take += __shfl_xor_sync(0xFFFFFFFFu, take, o);
-            return acc + take;
-        }
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-        acc += v;
-        end -= 32;
-    }
-    return acc;
-}
-
-// The same over 128-tile windows: lane l covers tiles [end-128+4l, +4). One
-// window costs one round trip to L2, so the walk keeps up with tiles that
-// finish faster than 32 per round trip.
-__device__ __forceinline__ uint32_t lb_sum_exclusive_wide(const uint64_t *status, uint32_t tile, uint32_t *err,
-                                                          uint32_t stride = 1) {
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t acc = 0;
-    int64_t end = (int64_t)tile;  // window is [end-128, end)
-    while (end > 0) {
-        int64_t base = end - 128 + 4 * (int64_t)lane;
-        uint64_t w[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            int64_t idx = base + i;
-            w[i] = idx >= 0 ? ld_relaxed_u64(status + idx * stride) : LB_PREFIX;
-        }
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            int64_t idx = base + i;
-            if (!(w[i] & LB_STATUS_MASK)) w[i] = lb_wait(status + idx * stride, err);
-        }
-        // highest tile of mine holding a prefix (-1: none)
-        int hi_mine = -1;
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-            if ((w[i] & LB_STATUS_MASK) == LB_PREFIX) hi_mine = i;
-        uint32_t lanes_with_prefix = __ballot_sync(0xFFFFFFFFu, hi_mine >= 0);
-        uint32_t v = 0;
-        if (lanes_with_prefix) {
-            int hl = 31 - __clz(lanes_with_prefix);  // lane holding the nearest prefix
-            if ((int)lane > hl) {
-#pragma unroll
-                for (int i = 0; i < 4; i++) v += (uint32_t)w[i];
-            } else if ((int)lane == hl) {
-#pragma unroll
-                for (int i = 0; i < 4; i++)
-                    if (i >= hi_mine) v += (uint32_t)w[i];
-            }
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-            return acc + v;
-        }
-#pragma unroll
-        for (int i = 0; i < 4; i++) v += (uint32_t)w[i];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-        acc += v;
-        end -= 128;
-    }
-    return acc;
-}
-
-// Per-lane look-back for lanes that each carry an independent value chain
-// (one value per tile per lane at status + tile*stride + lane). `op` combines
-// an older tile's value into the running value; walking stops at the first
-// PREFIX word. Each lane walks alone, so lanes may mix statuses safely.
-template <class Op>
-__device__ __forceinline__ uint32_t lb_lane_exclusive(const uint64_t *status, uint32_t tile, uint32_t stride,
-                                                      uint32_t identity, uint32_t *err, Op op) {
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t acc = identity;
-    for (int64_t t = (int64_t)tile - 1; t >= 0; t--) {
-        uint64_t w = lb_wait(status + (uint64_t)t * stride + lane, err);
-        acc = op((uint32_t)w, acc);
-        if ((w & LB_STATUS_MASK) == LB_PREFIX) break;
-    }
-    return acc;
 }
 
 // ------------------------------------------------------------ byte SWAR ----

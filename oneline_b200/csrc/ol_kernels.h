@@ -235,6 +235,9 @@ struct DictMatchArgs {
     const DictChain *chains;
     uint32_t n_chains;
     uint32_t chain_bytes;
+    // Test hook (ol_ctx_inject): each block takes its wait-timeout branch
+    // after its filter copy has landed, as if the bounded wait had run out.
+    uint32_t force_timeout;
 };
 
 cudaError_t launch_dict_match(const DictMatchArgs &a, int sm_count, cudaStream_t st, uint32_t slice = 512,

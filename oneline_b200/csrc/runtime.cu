@@ -176,6 +176,14 @@ extern "C" ol_status ol_ctx_sync(ol_ctx *ctx) {
 
 extern "C" void *ol_ctx_stream(ol_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
+extern "C" ol_status ol_ctx_inject(ol_ctx *ctx, uint32_t faults) {
+    if (!ctx) return OL_ERR_INVALID_ARG;
+    if (faults & ~(uint32_t)OL_INJECT_DICT_WAIT_TIMEOUT) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "unknown fault flag");
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    ctx->inject = faults;
+    return OL_OK;
+}
+
 // --------------------------------------------------------------- upload ----
 
 namespace ol {
@@ -263,7 +271,6 @@ ol_status parse_doc(ol_ctx *ctx, ol_doc *d, uint64_t est_lines, FlatNode **nodes
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "parse");
         const DocStats &hs = d->host_stats;
-        if (hs.error & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "parse: a bounded device wait ran out");
         if (hs.error & OL_DEVERR_FIXUP) return ctx_fail(ctx, OL_ERR_CUDA, "parse: fix-up list overflow");
         if (hs.error & OL_DEVERR_CAPACITY) {
             est_lines = hs.line_count;  // exact now

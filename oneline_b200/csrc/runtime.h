@@ -24,12 +24,10 @@ struct DevBuf {
     void release(cudaStream_t st);
 };
 
-// Small per-context device counters for searches and trees.
+// Small per-context device words (a status word read back by the tree build).
 struct CtxCounters {
-    uint32_t ticket;
-    uint32_t total;
     uint32_t error;
-    uint32_t pad[13];
+    uint32_t pad[15];
 };
 
 }  // namespace ol
@@ -49,6 +47,7 @@ struct ol_ctx {
     ol::DevBuf parse_slot;    // staged parse lines, 4 KiB per text tile
     ol_tuning tune{512, 0, 512, 1};  // kernel variants in use (ol_autotune / ol_tuning_set)
     uint64_t dict_stats[6] = {0, 0, 0, 0, 0, 0};  // the last dictionary search (ol_dict_stats)
+    uint32_t inject = 0;  // OL_INJECT_* faults armed for the next operation they name (ol_ctx_inject)
     ol::DevBuf pattern_dev;
     ol::DevBuf dict_small;   // dictionary search: per-pattern counts, ranks, slots
     ol::DevBuf dict_bitmap;  // heavy-pattern bitmaps

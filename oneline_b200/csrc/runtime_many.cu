@@ -332,6 +332,9 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
     ma.seg_start = seg_start;
     ma.seg_end = seg_end;
     ma.n_seg = n_seg;
+    // an armed injected timeout is taken by this search's first match pass
+    ma.force_timeout = (ctx->inject & OL_INJECT_DICT_WAIT_TIMEOUT) ? 1u : 0u;
+    ctx->inject &= ~OL_INJECT_DICT_WAIT_TIMEOUT;
     e = cudaMemsetAsync(m.sample_counts, 0, (size_t)U * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(m.light_n, 0, 16, st);
     if (e == cudaSuccess) e = launch_dict_match(ma, ctx->sm_count, st, ctx->tune.dict_slice, ctx->tune.dict_blocks_per_sm);
@@ -405,6 +408,7 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
         if (e == cudaSuccess) e = cudaMemsetAsync(m.light_n, 0, 16, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(m.stats, 0, 16, st);
         ma.stats = m.stats;
+        ma.force_timeout = 0;
         ma.tile_stride = 1;
         ma.count_only = 0;
         ma.counts = m.light_count;

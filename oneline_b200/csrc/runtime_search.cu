@@ -21,7 +21,7 @@ namespace {
 // the staged limit: one per launch). Results stay on the device: d_totals[i]
 // and d_outs[i]. Pattern bytes are copied to device memory first.
 cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pats, const uint32_t *lens, uint32_t n,
-                          const uint32_t *max_out, uint32_t *d_totals, uint32_t *const *d_outs, uint32_t *d_error) {
+                          const uint32_t *max_out, uint32_t *d_totals, uint32_t *const *d_outs) {
     cudaStream_t st = ctx->stream;
     uint32_t n_tiles = (uint32_t)((d->text_len + kSearchTile - 1) / kSearchTile);
     size_t total_bytes = 0;
@@ -145,16 +145,11 @@ ol_status search_multi_host(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *
     }
     for (size_t c = 0; c < idx.size(); c += 64) {
         uint32_t cn = (uint32_t)std::min<size_t>(64, idx.size() - c);
-        e = cudaMemsetAsync(&ctx->counters->error, 0, 4, st);
-        if (e == cudaSuccess)
-            e = enqueue_multi(ctx, d, p2.data() + c, l2.data() + c, cn, m2.data() + c, d_totals, o2.data() + c,
-                              &ctx->counters->error);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->host_counters, ctx->counters, sizeof(CtxCounters), cudaMemcpyDeviceToHost, st);
+        e = enqueue_multi(ctx, d, p2.data() + c, l2.data() + c, cn, m2.data() + c, d_totals, o2.data() + c);
         uint32_t tot_h[64];
         if (e == cudaSuccess) e = cudaMemcpyAsync(tot_h, d_totals, cn * 4, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "search");
-        if (ctx->host_counters->error & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "search: a bounded device wait ran out");
         for (uint32_t j = 0; j < cn; j++) {
             uint32_t i = idx[c + j];
             totals[i] = tot_h[j];
@@ -246,7 +241,7 @@ extern "C" ol_status ol_search_multi_async(ol_ctx *ctx, const ol_doc *d, const u
         size_t b = a + 1;
         while (b < map.size() && map[b] == map[b - 1] + 1) b++;
         cudaError_t e = enqueue_multi(ctx, d, p2.data() + a, l2.data() + a, (uint32_t)(b - a), m2.data() + a,
-                                      d_totals + map[a], o2.data() + a, &ctx->counters->error);
+                                      d_totals + map[a], o2.data() + a);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "search");
         a = b;
     }

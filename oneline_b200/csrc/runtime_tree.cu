@@ -110,7 +110,6 @@ ol_status build(ol_ctx *ctx, const ol_doc *d, ol_tree *t, uint32_t flags, bool w
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "tree");
     err = ctx->host_counters->error;
-    if (err & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "tree: a bounded device wait ran out");
     if (err & OL_DEVERR_DEEP) return ctx_fail(ctx, OL_ERR_CUDA, "tree: depth above the fast path reached the kernels");
     return OL_OK;
 }

@@ -83,6 +83,10 @@ def lib():
         L.olb_many_find_all_par.argtypes = [ctypes.c_void_p, u8p, u64, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_void_p, u64, ctypes.c_int]
         L.olb_many_find_all_par.restype = u64
+        L.olb_many_digest_par.argtypes = [ctypes.c_void_p, u8p, u64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.olb_many_digest_par.restype = u64
+        L.olb_hit_digest.argtypes = [u64, ctypes.c_uint32, ctypes.c_uint32]
+        L.olb_hit_digest.restype = u64
         _lib = L
     return _lib
 
@@ -180,6 +184,11 @@ def find_all(text, pattern: bytes) -> np.ndarray:
     return out[:total]
 
 
+def hit_digest(slot: int, pattern: int, offset: int) -> int:
+    """The per-hit term of CpuMany.digest_par (for checking other implementations of it)."""
+    return int(lib().olb_hit_digest(slot, pattern, offset))
+
+
 def _pack(patterns) -> tuple:
     lens = np.array([len(x) for x in patterns], np.uint32)
     blob = b"".join(bytes(x) for x in patterns)
@@ -208,9 +217,14 @@ class CpuBaseline:
     def __init__(self, threads: int | None = None):
         self.threads = int(threads or os.cpu_count() or 1)
 
+    def line_count(self, text) -> int:
+        """Lines of the text, counted per chunk in parallel (the count pass of parse_par)."""
+        p, n, _k = _buf(text)
+        return int(lib().olb_parse_par(p, n, 0, 0, 0, self.threads)) if n else 0
+
     def parse_par(self, text) -> tuple:
         p, n, _k = _buf(text)
-        cap = lib().olo_count_lines(p, n) if n else 0
+        cap = self.line_count(text)
         offs = np.zeros(max(cap, 1), np.uint32)
         nodes = np.zeros(max(cap, 1), NODE_DTYPE)
         got = lib().olb_parse_par(p, n, _ptr(offs), _ptr(nodes), cap, self.threads)
@@ -218,6 +232,7 @@ class CpuBaseline:
         return offs[:cap], nodes[:cap]
 
     def parse_par_into(self, text_ptr: int, n: int, offs: np.ndarray, nodes: np.ndarray) -> int:
+        """parse_par into caller-sized outputs (ParseBuffers reuse, lib.rs:445-469); returns the line count."""
         return lib().olb_parse_par(text_ptr, n, _ptr(offs), _ptr(nodes), offs.size, self.threads)
 
     def build_links(self, nodes: np.ndarray, out: dict | None = None) -> dict:
@@ -262,6 +277,16 @@ class CpuMany:
         total = lib().olb_many_find_all_par(self._h, p, n, _ptr(counts), _ptr(hp), _ptr(ho), cap, self.threads)
         k = min(total, cap)
         return counts[: self.n], hp[:k], ho[:k], total
+
+    def digest_par(self, text) -> tuple:
+        """(counts u64[n], total, digest): the per-pattern counts and the order-checking
+        digest of the whole (pattern, offset)-ordered hit list (hit_digest summed over
+        the slots), without materialising the list."""
+        p, n, _k = _buf(text)
+        counts = np.zeros(max(self.n, 1), np.uint64)
+        total = ctypes.c_uint64()
+        dg = lib().olb_many_digest_par(self._h, p, n, _ptr(counts), ctypes.addressof(total), self.threads)
+        return counts[: self.n], int(total.value), int(dg)
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -255,6 +255,19 @@ void nearest_previous(const uint32_t *keys, size_t n, bool or_equal, uint32_t *r
     });
 }
 
+// Equality of n bytes; n <= 8 as one masked 64-bit compare (the caller
+// guarantees 8 readable bytes at both addresses), longer ones with memcmp.
+inline bool same_bytes(const uint8_t *a, const uint8_t *b, size_t n) {
+    if (n <= 8) {
+        uint64_t x, y;
+        memcpy(&x, a, 8);
+        memcpy(&y, b, 8);
+        uint64_t mask = n == 8 ? ~0ull : ((1ull << (8 * n)) - 1);
+        return ((x ^ y) & mask) == 0;
+    }
+    return memcmp(a, b, n) == 0;
+}
+
 // First/last-byte AVX2 filter + memcmp: every overlapping occurrence of p in
 // hay[0..len), reported as base + i.
 __attribute__((target("avx2,bmi"))) void find_chunk_avx2(const uint8_t *hay, size_t len, const uint8_t *p, size_t m,
@@ -265,13 +278,20 @@ __attribute__((target("avx2,bmi"))) void find_chunk_avx2(const uint8_t *hay, siz
     if (m >= 2) {
         const __m256i f = _mm256_set1_epi8((char)p[0]);
         const __m256i l = _mm256_set1_epi8((char)p[m - 1]);
+        // pattern bytes 1..m-2, padded so that the short compare may read 8
+        uint8_t mid[8] = {0};
+        memcpy(mid, p + 1, std::min<size_t>(m - 2, 8));
+        const bool short_mid = m - 2 <= 8;
         for (; i + 32 <= last + 1; i += 32) {
             __m256i a = _mm256_loadu_si256((const __m256i *)(hay + i));
             __m256i b = _mm256_loadu_si256((const __m256i *)(hay + i + m - 1));
             uint32_t mask = (uint32_t)_mm256_movemask_epi8(_mm256_and_si256(_mm256_cmpeq_epi8(a, f), _mm256_cmpeq_epi8(b, l)));
             while (mask) {
                 size_t k = i + (size_t)__builtin_ctz(mask);
-                if (memcmp(hay + k + 1, p + 1, m - 2) == 0) out.push_back((uint32_t)(base + k));
+                // 8 bytes from k + 1 stay inside hay when k + 1 + 8 <= len
+                bool eq = short_mid && k + 9 <= len ? same_bytes(hay + k + 1, mid, m - 2)
+                                                    : memcmp(hay + k + 1, p + 1, m - 2) == 0;
+                if (eq) out.push_back((uint32_t)(base + k));
                 mask &= mask - 1;
             }
         }
@@ -397,14 +417,15 @@ uint64_t olb_find_all_par(const uint8_t *text, uint64_t len, const uint8_t *pat,
         size_t wend = std::min<size_t>(end + m - 1, len);
         find_chunk(text + start, wend - start, pat, m, start, parts[c]);
     });
-    uint64_t total = 0;
-    for (auto &p : parts) {
-        for (uint32_t v : p) {
-            if (total < cap) out[total] = v;
-            total++;
-        }
-    }
-    return total;
+    // chunks in order; each copies its hits to its place in parallel
+    std::vector<uint64_t> at(nch + 1, 0);
+    for (size_t c = 0; c < nch; c++) at[c + 1] = at[c] + parts[c].size();
+    parallel_for(threads, nch, [&](size_t c) {
+        if (at[c] >= cap || parts[c].empty()) return;
+        size_t k = (size_t)std::min<uint64_t>(parts[c].size(), cap - at[c]);
+        memcpy(out + at[c], parts[c].data(), k * 4);
+    });
+    return at[nch];
 }
 
 // ManyPatterns::new (search.rs:214-227): Aho-Corasick automaton, MatchKind::Standard.
@@ -547,6 +568,81 @@ uint64_t olb_many_find_all_par(void *p, const uint8_t *text, uint64_t len, uint6
             }
     }
     return total;
+}
+
+// Order-checking digest of the whole sorted hit list, without building it:
+// the sum over every hit of hit_digest(slot, pattern, offset), where slot is
+// the hit's index in the (pattern, offset) order of ManyPatterns::find_all_par
+// (search.rs:259-282). Two passes over the same chunks: the first counts each
+// pattern's hits per chunk; the second walks again and, since a chunk meets a
+// pattern's hits in ascending offset order, gives each its slot from the
+// running per-(chunk, pattern) base. counts[i] receives pattern i's hits.
+// Returns the digest; *total the number of hits.
+uint64_t olb_hit_digest(uint64_t slot, uint32_t pattern, uint32_t offset) {
+    uint64_t x = (((uint64_t)pattern << 32) | offset) ^ (slot * 0x9E3779B97F4A7C15ull);
+    x ^= x >> 30;
+    x *= 0xBF58476D1CE4E5B9ull;
+    x ^= x >> 27;
+    x *= 0x94D049BB133111EBull;
+    x ^= x >> 31;
+    return x;
+}
+
+uint64_t olb_many_digest_par(void *p, const uint8_t *text, uint64_t len, uint64_t *counts, uint64_t *total_out,
+                             int threads) {
+    const AcDfa &d = *(const AcDfa *)p;
+    const uint32_t np = (uint32_t)d.lens.size();
+    for (uint32_t i = 0; i < np; i++) counts[i] = 0;
+    *total_out = 0;
+    if (len == 0 || np == 0) return 0;
+    size_t chunk = std::max<size_t>(len / ((size_t)threads * 4), 1 << 20);
+    size_t nch = (len + chunk - 1) / chunk;
+    const uint32_t nc = d.n_classes;
+    // walk(c, f): f(pattern, offset) for every hit starting in chunk c, in the
+    // order the automaton meets them
+    auto walk = [&](size_t c, auto &&f) {
+        size_t start = c * chunk, end = std::min<size_t>(start + chunk, len);
+        size_t wend = std::min<size_t>(end + d.longest - 1, len);
+        uint32_t s = 0;
+        const uint32_t *tr = d.trans.data();
+        for (size_t i = start; i < wend; i++) {
+            s = tr[(size_t)s * nc + d.cls[text[i]]];
+            uint32_t st = d.out_first[s] != NONE ? s : d.out_link[s];
+            while (st != NONE) {
+                for (uint32_t id = d.out_first[st]; id != NONE; id = d.pid_next[id]) {
+                    size_t mstart = i + 1 - d.lens[id];
+                    if (mstart >= start && mstart < end) f(id, (uint32_t)mstart);
+                }
+                st = d.out_link[st];
+            }
+        }
+    };
+    std::vector<std::vector<uint64_t>> per(nch, std::vector<uint64_t>(np, 0));
+    parallel_for(threads, nch, [&](size_t c) {
+        auto &cnt = per[c];
+        walk(c, [&](uint32_t id, uint32_t) { cnt[id]++; });
+    });
+    // per-(chunk, pattern) first slot: patterns in order, chunks in order within each
+    uint64_t at = 0;
+    for (uint32_t i = 0; i < np; i++) {
+        for (size_t c = 0; c < nch; c++) {
+            uint64_t k = per[c][i];
+            per[c][i] = at;
+            at += k;
+            counts[i] += k;
+        }
+    }
+    *total_out = at;
+    std::vector<uint64_t> sums(nch, 0);
+    parallel_for(threads, nch, [&](size_t c) {
+        auto &next = per[c];
+        uint64_t sum = 0;
+        walk(c, [&](uint32_t id, uint32_t off) { sum += olb_hit_digest(next[id]++, id, off); });
+        sums[c] = sum;
+    });
+    uint64_t digest = 0;
+    for (uint64_t v : sums) digest += v;
+    return digest;
 }
 
 }  // extern "C"

@@ -1,6 +1,7 @@
 """Host-side pieces of the benchmark that run without a GPU: the DRAM traffic
-figure the roofline reports comes from the committed ncu summary, and the
-reference arm's line keeps the contract's keys."""
+figure the roofline reports comes from the committed ncu summary, the
+reference arm's line keeps the contract's keys and times the GPU line's
+config, and the parity checkers find differences."""
 import json
 import subprocess
 import sys
@@ -31,3 +32,39 @@ def test_reference_arm_prints_one_contract_line():
     assert d["impl"] == "reference" and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] in ("reference", "port")
+    assert d["config"]["text_bytes"] == 64 << 20  # the whole document, the GPU line's config
+    assert set(d["cpu_baseline"]["stage_ms"]) == {"parse_par", "build_links", "find_all_par"}
+
+
+def test_first_mismatch_names_the_first_difference():
+    import numpy as np
+
+    a = np.arange(10, dtype=np.uint32)
+    assert bench.first_mismatch("x", a, a.copy()) is None
+    b = a.copy()
+    b[7] = 0
+    b[9] = 1
+    assert bench.first_mismatch("x", b, a) == "x[7]: 0 vs 7 (2 differ)"
+    assert "entries" in bench.first_mismatch("x", a[:5], a)
+
+
+def test_device_hit_digest_equals_the_cpu_ports_digest():
+    """The checker's torch digest (run here on a CPU tensor) of the oracle's sorted
+    hit list equals the CPU port's digest, and a swapped pair changes it."""
+    import numpy as np
+    import torch
+
+    import oracle
+    from oneline_b200 import datagen
+
+    text = datagen.corpus(1 << 20, 8)
+    pats = datagen.patterns_dictionary(text, 8, n=100)
+    counts, hp, ho = oracle.find_many(text, pats)
+    hits = np.empty(2 * len(hp), np.uint32)
+    hits[0::2], hits[1::2] = hp, ho
+    t = torch.from_numpy(hits.view(np.int32).copy())
+    _, total, dg = oracle.CpuBaseline(threads=2).many(pats).digest_par(text)
+    assert total == len(hp)
+    assert bench.device_hit_digest(t, total, chunk=1000) == dg
+    hits[2:4], hits[4:6] = hits[4:6].copy(), hits[2:4].copy()
+    assert bench.device_hit_digest(torch.from_numpy(hits.view(np.int32).copy()), total) != dg

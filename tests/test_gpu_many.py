@@ -146,3 +146,23 @@ def test_runs_of_one_byte(parser, heavy_min_hits):
     pats += [b"|" * k + b"-" for k in (4, 12)] + [b"a|||", b"||||a|||"]
     assert_many_device(parser, text, pats, heavy_min_hits, what=f"heavy >= {heavy_min_hits}")
     assert_many(parser, text, pats, what="host hits")
+
+
+def test_injected_wait_timeout_is_reported_and_leaves_the_context_usable(parser):
+    """The dictionary kernel's one bounded wait (its filter's bulk copy), made to
+    run out on the host's word (ol_ctx_inject), after the copy has landed: the
+    call fails with OL_ERR_TIMEOUT and the next search on the same context and
+    document is exact. Nothing on the GPU faults or hangs."""
+    from oneline_b200 import _lib
+
+    text = datagen.corpus(1 << 20, 21).tobytes()
+    pats = [text[1000:1008], b"||||", b"zzzzzz", text[-20:-4]]
+    doc = parser.upload(text)
+    ps = parser.compile_patterns(doc, pats)
+    L = _lib.load()
+    assert L.ol_ctx_inject(parser.ctx, 0xFF) == 1  # unknown flags are refused
+    assert L.ol_ctx_inject(parser.ctx, 1) == 0
+    with pytest.raises(OnelineError) as ei:
+        parser.search_many(doc, ps, 1 << 20)
+    assert ei.value.status == 7 and "bounded wait" in str(ei.value), ei.value
+    assert_many(parser, text, pats, what="after the injected timeout")

@@ -158,3 +158,27 @@ def test_cpu_baseline_dictionary_matches_oracle():
     c2, hp2, ho2, total = m.find_all_par(text)
     assert total == len(hp)
     assert np.array_equal(counts, c2) and np.array_equal(hp, hp2) and np.array_equal(ho, ho2)
+
+
+def test_cpu_baseline_dictionary_digest_matches_the_sorted_hit_list():
+    """The order-checking digest (counts + sum of hit_digest over slots), computed
+    without building the list, equals the digest of the oracle's sorted list."""
+    text = datagen.corpus(1 << 20, 6)
+    pats = datagen.patterns_dictionary(text, 6, n=200) + [b"||||", b"||||"]
+    counts, hp, ho = oracle.find_many(text, pats)
+    m = oracle.CpuBaseline(threads=4).many(pats)
+    c2, total, dg = m.digest_par(text)
+    assert total == len(hp) and np.array_equal(c2, counts)
+    slots = np.arange(len(hp), dtype=np.uint64)
+    x = (hp.astype(np.uint64) << np.uint64(32) | ho.astype(np.uint64)) ^ (slots * np.uint64(0x9E3779B97F4A7C15))
+    x ^= x >> np.uint64(30)
+    x *= np.uint64(0xBF58476D1CE4E5B9)
+    x ^= x >> np.uint64(27)
+    x *= np.uint64(0x94D049BB133111EB)
+    x ^= x >> np.uint64(31)
+    assert int(x.sum(dtype=np.uint64)) == dg
+    assert oracle.hit_digest(5, int(hp[5]), int(ho[5])) == int(x[5])
+    # a swap of two hits changes the digest
+    y = np.array([oracle.hit_digest(i, int(hp[i]), int(ho[i])) for i in (0, 1)], np.uint64)
+    z = np.array([oracle.hit_digest(i, int(hp[1 - i]), int(ho[1 - i])) for i in (0, 1)], np.uint64)
+    assert int(y.sum(dtype=np.uint64)) != int(z.sum(dtype=np.uint64))

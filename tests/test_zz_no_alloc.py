@@ -130,3 +130,33 @@ def test_refusals_are_clear_and_leave_it_usable(parser):
     assert s == OL_ERR_INVALID_ARG and "16-byte" in msg, msg
     torch.cuda.synchronize()
     check_pair(parser, [(text, b"| ", 1 << 16), (text, text[500:520], 4)])
+
+
+def test_pinned_pattern_buffer_reused_at_once(parser):
+    """The pattern's bytes are taken during the call: a caller that overwrites a
+    pinned pattern buffer right after the call returns still gets the results
+    of the pattern it passed."""
+    import torch
+
+    L = _lib.load()
+    text = datagen.corpus((2 << 20) + 99, 15).tobytes()
+    d_text, cap = device_text(text, b"#")
+    first, second = text[4096:4100], text[70_001:70_013]
+    pin = torch.empty(64, dtype=torch.uint8, pin_memory=True)
+    stream = torch.cuda.current_stream()
+    got = []
+    for pattern in (first, second):
+        pin.numpy()[: len(pattern)] = np.frombuffer(pattern, np.uint8)
+        d_total = torch.zeros(1, dtype=torch.int32, device="cuda")
+        d_out = torch.zeros(1 << 16, dtype=torch.int32, device="cuda")
+        err = ctypes.create_string_buffer(256)
+        s = L.ol_search_noalloc(d_text.data_ptr(), len(text), cap, pin.data_ptr(), len(pattern), 1 << 16,
+                                d_total.data_ptr(), d_out.data_ptr(), stream.cuda_stream, err, len(err))
+        assert s == 0, err.value.decode()
+        pin.numpy()[:] = 0x7E  # overwritten before the GPU has run the search
+        stream.synchronize()
+        total = int(d_total.cpu().numpy().view(np.uint32)[0])
+        got.append((total, d_out[: min(total, 1 << 16)].cpu().numpy().view(np.uint32).copy()))
+    for pattern, (total, offs) in zip((first, second), got):
+        want_total, want_offs = expect(parser, text, pattern, 1 << 16)
+        assert total == want_total and np.array_equal(offs, want_offs), pattern
