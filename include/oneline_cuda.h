@@ -95,6 +95,36 @@ ol_status ol_ctx_inject(ol_ctx *ctx, uint32_t faults);
  * launch counts itself). For benchmarks; no reference counterpart. */
 uint64_t ol_launch_count(void);
 
+/* ---- profiling: StageTimer / Profile (crates/oneline-gpu/src/timing.rs:16-124)
+ *      behind GpuParser::profile_upload, profile_query_document
+ *      (document.rs:136-157), profile_search_document, profile_search_raw
+ *      (search.rs:143-173), profile_search_many (many.rs:401-410),
+ *      profile_build_tree, profile_build_tree_reusing (tree.rs:69-82) and
+ *      profile_query_raw (query.rs:275). Between ol_profile_begin and
+ *      ol_profile_end every GPU pass the context enqueues (upload copy, parse,
+ *      tree, search, dictionary stages, query, download) is timed by CUDA
+ *      events on its stream, and every blocking step marks the host time spent
+ *      since the previous mark. ol_profile_end waits for the stream and fills
+ *      *out: wall_ns is the host time from begin to the last mark,
+ *      gpu_total_ns the sum of the passes (Profile::gpu_total). At most
+ *      OL_PROFILE_MAX_STEPS of each are kept. */
+#define OL_PROFILE_MAX_STEPS 32
+#define OL_PROFILE_LABEL_LEN 40
+typedef struct ol_profile_step {
+    char label[OL_PROFILE_LABEL_LEN];
+    uint64_t ns;
+} ol_profile_step;
+typedef struct ol_profile {
+    uint64_t wall_ns;
+    uint64_t gpu_total_ns;
+    uint32_t n_host_steps;
+    uint32_t n_gpu_passes;
+    ol_profile_step host_steps[OL_PROFILE_MAX_STEPS];
+    ol_profile_step gpu_passes[OL_PROFILE_MAX_STEPS];
+} ol_profile;
+ol_status ol_profile_begin(ol_ctx *ctx);
+ol_status ol_profile_end(ol_ctx *ctx, ol_profile *out);
+
 /* ---- resident documents: GpuParser::upload, GpuDocument::{line_count,text_len}
  *      (crates/oneline-gpu/src/document.rs:16-90, 111-127) */
 ol_status ol_doc_upload(ol_ctx *ctx, const uint8_t *text, uint64_t len, ol_doc **out);
@@ -251,6 +281,17 @@ ol_status ol_search_many(ol_ctx *ctx, const ol_doc *doc, const ol_patset *set, u
  * keys (0: automatic). It changes the speed, never the result. */
 ol_status ol_search_many_device(ol_ctx *ctx, const ol_doc *doc, const ol_patset *set, uint64_t max_hits,
                                 uint32_t heavy_min_hits, uint32_t *counts, uint64_t *total_hits, ol_hit *d_hits);
+/* The same results in the hit form the north-star workload states, (pattern
+ * id u32, byte offset u64): hit i is (patterns[i], offsets[i]), two arrays of
+ * max_hits entries, in (pattern, offset) order. It extends ManyHit's u32
+ * offset (crates/oneline-gpu/src/many.rs:77-82) to 64 bits; the values are
+ * the same. ol_search_many_u64 writes host arrays; ol_search_many_device_u64
+ * device arrays (d_offsets 8-byte aligned). */
+ol_status ol_search_many_u64(ol_ctx *ctx, const ol_doc *doc, const ol_patset *set, uint64_t max_hits, uint32_t *counts,
+                             uint64_t *total_hits, uint32_t *patterns, uint64_t *offsets);
+ol_status ol_search_many_device_u64(ol_ctx *ctx, const ol_doc *doc, const ol_patset *set, uint64_t max_hits,
+                                    uint32_t heavy_min_hits, uint32_t *counts, uint64_t *total_hits,
+                                    uint32_t *d_patterns, uint64_t *d_offsets);
 /* Work of the last dictionary search on ctx, for tuning and reports: out[0]
  * text bytes, [1] positions walked in the trie (filter and table hits), [2] trie
  * nodes visited, [3] patterns collected as bitmaps, [4] hits collected as sorted

@@ -22,6 +22,7 @@ from .gpu import (  # noqa: F401
     GpuPipeline,
     GpuTree,
     ManyResult,
+    Profile,
     QueryResult,
     SearchResult,
 )

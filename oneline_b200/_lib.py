@@ -37,6 +37,8 @@ SIGNATURES: dict[str, tuple] = {
     "ol_ctx_stream": (_P, [_P]),
     "ol_ctx_inject": (_S, [_P, _U32]),
     "ol_launch_count": (_U64, []),
+    "ol_profile_begin": (_S, [_P]),
+    "ol_profile_end": (_S, [_P, _P]),
     "ol_doc_upload": (_S, [_P, _U8P, _U64, _PP]),
     "ol_doc_upload_device": (_S, [_P, _U8P, _U64, _PP]),
     "ol_doc_free": (None, [_P]),
@@ -83,6 +85,8 @@ SIGNATURES: dict[str, tuple] = {
     "ol_patset_unique": (_U32, [_P]),
     "ol_search_many": (_S, [_P, _P, _P, _U64, _P, _U64P, _P]),
     "ol_search_many_device": (_S, [_P, _P, _P, _U64, _U32, _P, _U64P, _P]),
+    "ol_search_many_u64": (_S, [_P, _P, _P, _U64, _P, _U64P, _P, _P]),
+    "ol_search_many_device_u64": (_S, [_P, _P, _P, _U64, _U32, _P, _U64P, _P, _P]),
     "ol_batch_upload": (_S, [_P, _U8P, _P, _U32, _PP]),
     "ol_batch_free": (None, [_P]),
     "ol_batch_docs": (_U32, [_P]),

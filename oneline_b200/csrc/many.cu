@@ -594,6 +594,19 @@ cudaError_t launch_dict_ids(const DictEmitArgs &a, cudaStream_t st) {
 
 // ----------------------------------------------------------------- emit ----
 
+// One hit into output slot `slot`: a ManyHit {pattern, offset u32}, or the
+// (pattern u32, offset u64) pair of arrays. Streaming stores: the emission
+// never reads them back.
+__device__ __forceinline__ void put_hit(const DictEmitArgs &a, unsigned long long slot, uint32_t id, uint32_t off) {
+    if (slot >= a.max_hits) return;
+    if (a.hit_off) {
+        __stcs(a.hit_pat + slot, id);
+        __stcs(a.hit_off + slot, (unsigned long long)off);
+    } else {
+        __stcs(&a.hits[slot], make_uint2(id, off));
+    }
+}
+
 // Heavy hits: block (b, h) expands words [4096b, 4096b + 4096) of bitmap h,
 // warp w the 512 words [4096b + 512w, ...), 32 words per round. Each lane
 // lists its word's hits, at their ranks from a warp scan of the popcounts, in
@@ -664,15 +677,11 @@ __global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArg
             if (j < T) {
                 const uint32_t off = buf[j];
                 if (cached) {
-                    for (uint32_t d = 0; d < n_dup; d++) {
-                        const unsigned long long slot = dup_base[d] + rank + j;
-                        if (slot < a.max_hits) __stcs(&a.hits[slot], make_uint2(dup_id[d], off));  // streamed: never re-read here
-                    }
+                    for (uint32_t d = 0; d < n_dup; d++) put_hit(a, dup_base[d] + rank + j, dup_id[d], off);
                 } else {
                     for (uint32_t d = d0; d < d1; d++) {
                         const uint32_t id = __ldg(a.dup_ids + d);
-                        const unsigned long long slot = a.id_base[id] + rank + j;
-                        if (slot < a.max_hits) a.hits[slot] = make_uint2(id, off);
+                        put_hit(a, a.id_base[id] + rank + j, id, off);
                     }
                 }
             }
@@ -691,8 +700,7 @@ __global__ void dict_emit_light_kernel(DictEmitArgs a) {
     const uint32_t d0 = a.dup_start[u], d1 = a.dup_start[u + 1];
     for (uint32_t d = d0; d < d1; d++) {
         const uint32_t id = a.dup_ids[d];
-        const unsigned long long slot = a.id_base[id] + rank;
-        if (slot < a.max_hits) a.hits[slot] = make_uint2(id, off);
+        put_hit(a, a.id_base[id] + rank, id, off);
     }
 }
 

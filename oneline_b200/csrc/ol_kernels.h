@@ -273,6 +273,10 @@ struct DictEmitArgs {
     unsigned long long *total;
     uint2 *hits;                 // {pattern, offset}
     unsigned long long max_hits;
+    // The (pattern u32, offset u64) form: when hit_off is set, hits go to
+    // these two arrays instead of `hits`.
+    uint32_t *hit_pat;
+    unsigned long long *hit_off;
 };
 cudaError_t launch_dict_ids(const DictEmitArgs &a, cudaStream_t st);
 

@@ -155,6 +155,7 @@ extern "C" void ol_ctx_destroy(ol_ctx *ctx) {
         if (ctx->ring[i]) cudaFreeHost(ctx->ring[i]);
         if (ctx->ring_done[i]) cudaEventDestroy(ctx->ring_done[i]);
     }
+    prof_discard(ctx);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -192,6 +193,7 @@ namespace ol {
 // through the ring: the copy of chunk i+1 into a pinned slot overlaps the DMA
 // of chunk i (crates/oneline-gpu/src/staging.rs:59-117).
 cudaError_t h2d(ol_ctx *ctx, uint8_t *dev, const uint8_t *host, uint64_t len) {
+    GpuPass pass(ctx, "upload: copy to device");
     cudaPointerAttributes attr;
     cudaError_t e = cudaPointerGetAttributes(&attr, host);
     if (e == cudaSuccess && (attr.type == cudaMemoryTypeHost || attr.type == cudaMemoryTypeManaged))
@@ -210,6 +212,7 @@ cudaError_t h2d(ol_ctx *ctx, uint8_t *dev, const uint8_t *host, uint64_t len) {
 
 // Enqueues the parse of doc's resident text into its buffers.
 cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d) {
+    GpuPass pass(ctx, "parse");
     cudaStream_t st = ctx->stream;
     cudaError_t e;
     uint32_t n_tiles = parse_tiles(d->text_len);
@@ -343,11 +346,13 @@ static ol_status upload_common(ol_ctx *ctx, const uint8_t *text, uint64_t len, b
         e = h2d(ctx, d->text, text, len);
         est = estimate_lines(text, len);
     }
+    prof_mark(ctx, "upload: enqueue copy");
     if (e != cudaSuccess) {
         ol_doc_free(d);
         return ctx_cuda(ctx, e, "upload");
     }
     s = parse_doc(ctx, d, est, nullptr);
+    prof_mark(ctx, "upload: wait for parse");
     if (s != OL_OK) {
         ol_doc_free(d);
         return s;
@@ -395,8 +400,13 @@ static ol_status read_array(ol_ctx *ctx, const ol_doc *d, void *out, const void 
     if (d->line_count == 0) return OL_OK;
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
-    cudaError_t e = cudaMemcpyAsync(out, src, (size_t)d->line_count * elem, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaError_t e;
+    {
+        GpuPass pass(ctx, "download");
+        e = cudaMemcpyAsync(out, src, (size_t)d->line_count * elem, cudaMemcpyDeviceToHost, ctx->stream);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    prof_mark(ctx, "download");
     return ctx_cuda(ctx, e, "download");
 }
 

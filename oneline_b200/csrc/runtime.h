@@ -24,6 +24,8 @@ struct DevBuf {
     void release(cudaStream_t st);
 };
 
+struct Prof;
+
 // Small per-context device words (a status word read back by the tree build).
 struct CtxCounters {
     uint32_t error;
@@ -48,6 +50,7 @@ struct ol_ctx {
     ol_tuning tune{512, 0, 512, 1};  // kernel variants in use (ol_autotune / ol_tuning_set)
     uint64_t dict_stats[6] = {0, 0, 0, 0, 0, 0};  // the last dictionary search (ol_dict_stats)
     uint32_t inject = 0;  // OL_INJECT_* faults armed for the next operation they name (ol_ctx_inject)
+    ol::Prof *prof = nullptr;  // open profile (ol_profile_begin), or null
     ol::DevBuf pattern_dev;
     ol::DevBuf dict_small;   // dictionary search: per-pattern counts, ranks, slots
     ol::DevBuf dict_bitmap;  // heavy-pattern bitmaps
@@ -87,6 +90,21 @@ struct ol_tree {
 };
 
 namespace ol {
+// Profiling (profile.cu): a GPU pass is timed by CUDA events recorded on the
+// context's stream at construction and destruction, when a profile is open;
+// prof_mark ends a host step.
+struct GpuPass {
+    ol_ctx *ctx;
+    int index = -1;
+    GpuPass(ol_ctx *c, const char *label);
+    ~GpuPass() { done(); }
+    void done();  // ends the pass here instead of at destruction
+    GpuPass(const GpuPass &) = delete;
+    GpuPass &operator=(const GpuPass &) = delete;
+};
+void prof_mark(ol_ctx *ctx, const char *label);
+void prof_discard(ol_ctx *ctx);
+
 ol_status ctx_fail(ol_ctx *ctx, ol_status code, const std::string &msg);
 ol_status ctx_cuda(ol_ctx *ctx, cudaError_t e, const char *what);
 uint32_t parse_tiles(uint64_t len);
@@ -101,7 +119,16 @@ cudaError_t launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *hpa
                          uint32_t *const *d_outs);
 // Sets ctx->tune from the line for ctx's device in the tuning file at path.
 ol_status load_tuning(ol_ctx *ctx, const char *path);
+// Where a dictionary search puts its hits: ManyHits on the host or the device,
+// or the (pattern u32, offset u64) pair of arrays on the host or the device.
+struct HitDest {
+    ol_hit *host = nullptr;
+    ol_hit *dev = nullptr;
+    uint32_t *pat = nullptr;
+    uint64_t *off = nullptr;
+    bool pair_on_host = false;
+};
 ol_status many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits, uint32_t heavy_min_hits,
-                   uint32_t *counts, uint64_t *total, ol_hit *host_hits, ol_hit *d_hits,
+                   uint32_t *counts, uint64_t *total, const HitDest &dest,
                    const unsigned long long *seg_start, const unsigned long long *seg_end, uint32_t n_seg);
 }  // namespace ol

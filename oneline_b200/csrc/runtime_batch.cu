@@ -232,6 +232,8 @@ extern "C" ol_status ol_batch_search_many(ol_ctx *ctx, const ol_batch *b, const 
     if (b->ctx != ctx) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "batch belongs to another context");
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
-    return many_run(ctx, b->doc, set, max_hits, heavy_min_hits, counts, total_hits, nullptr, d_hits, b->seg_start,
+    HitDest dest;
+    dest.dev = d_hits;
+    return many_run(ctx, b->doc, set, max_hits, heavy_min_hits, counts, total_hits, dest, b->seg_start,
                     b->seg_end, b->n);
 }

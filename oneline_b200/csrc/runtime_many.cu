@@ -265,7 +265,7 @@ extern "C" uint32_t ol_patset_unique(const ol_patset *s) { return s ? s->n_u : 0
 // host_hits through ctx->dict_hits. counts (n_ids) and *total are host outputs.
 // seg_start/seg_end (device, n_seg): batches, whose hits stay inside a document.
 ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits, uint32_t heavy_min_hits,
-                       uint32_t *counts, uint64_t *total, ol_hit *host_hits, ol_hit *d_hits,
+                       uint32_t *counts, uint64_t *total, const HitDest &dest,
                        const unsigned long long *seg_start, const unsigned long long *seg_end, uint32_t n_seg) {
     cudaStream_t st = ctx->stream;
     const uint32_t n = set->n_ids, U = set->n_u;
@@ -337,12 +337,16 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
     ctx->inject &= ~OL_INJECT_DICT_WAIT_TIMEOUT;
     e = cudaMemsetAsync(m.sample_counts, 0, (size_t)U * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(m.light_n, 0, 16, st);
-    if (e == cudaSuccess) e = launch_dict_match(ma, ctx->sm_count, st, ctx->tune.dict_slice, ctx->tune.dict_blocks_per_sm);
+    if (e == cudaSuccess) {
+        GpuPass pass(ctx, "dictionary: sample counts");
+        e = launch_dict_match(ma, ctx->sm_count, st, ctx->tune.dict_slice, ctx->tune.dict_blocks_per_sm);
+    }
     std::vector<uint32_t> sample(U);
     uint32_t flags[2] = {0, 0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(sample.data(), m.sample_counts, (size_t)U * 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(flags, m.light_n, 8, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    prof_mark(ctx, "dictionary: wait for the sample");
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "search_many sample");
     if (flags[1] & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "search_many: a bounded wait ran out");
     const double scale = (double)n_tiles / (double)n_work;
@@ -421,9 +425,13 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
         ma.chains = m.chains;
         ma.n_chains = (uint32_t)chains.size();
         ma.chain_bytes = chain_bytes;
-        if (e == cudaSuccess) e = launch_dict_match(ma, ctx->sm_count, st, ctx->tune.dict_slice, ctx->tune.dict_blocks_per_sm);
+        if (e == cudaSuccess) {
+            GpuPass pass(ctx, "dictionary: match");
+            e = launch_dict_match(ma, ctx->sm_count, st, ctx->tune.dict_slice, ctx->tune.dict_blocks_per_sm);
+        }
         if (e == cudaSuccess) e = cudaMemcpyAsync(flags, m.light_n, 8, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        prof_mark(ctx, "dictionary: wait for the match pass");
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "search_many match");
         if (flags[1] & OL_DEVERR_TIMEOUT) return ctx_fail(ctx, OL_ERR_TIMEOUT, "search_many: a bounded wait ran out");
         light_n = flags[0];
@@ -433,6 +441,7 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
     }
 
     // 3. Heavy ranks, light order, per-id slots.
+    GpuPass order_pass(ctx, "dictionary: rank and sort");
     if (H) {
         e = launch_dict_heavy_count((const uint32_t *)ctx->dict_bitmap.ptr, n_words, H, m.heavy_counts, hld, st);
         if (e == cudaSuccess) e = launch_scan_columns(m.heavy_counts, m.heavy_bases, m.heavy_totals, hblocks, H, hld, st);
@@ -479,12 +488,14 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
     ea.id_base = m.id_base;
     ea.total = m.total;
     e = launch_dict_ids(ea, st);
+    order_pass.done();
     unsigned long long tot = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&tot, m.total, 8, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(counts, m.id_counts, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
     unsigned long long walk[2] = {0, 0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(walk, m.stats, 16, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    prof_mark(ctx, "dictionary: wait for the slots");
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "search_many ids");
     *total = tot;
     ctx->dict_stats[0] = N;
@@ -498,15 +509,37 @@ ol_status ol::many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint6
     const uint64_t k = std::min<uint64_t>(tot, max_hits);
     if (k == 0) return OL_OK;
     ea.max_hits = k;
-    if (d_hits) {
-        ea.hits = reinterpret_cast<uint2 *>(d_hits);
+    const size_t off_at = (k * 4 + 255) & ~(size_t)255;  // pair form in scratch: patterns, then offsets
+    if (dest.off && !dest.pair_on_host) {
+        ea.hit_pat = dest.pat;
+        ea.hit_off = reinterpret_cast<unsigned long long *>(dest.off);
+    } else if (dest.dev) {
+        ea.hits = reinterpret_cast<uint2 *>(dest.dev);
     } else {
-        if ((e = ctx->dict_hits.reserve(k * 8, st)) != cudaSuccess) return ctx_cuda(ctx, e, "search_many hits");
-        ea.hits = (uint2 *)ctx->dict_hits.ptr;
+        const size_t need = dest.off ? off_at + k * 8 : k * 8;
+        if ((e = ctx->dict_hits.reserve(need, st)) != cudaSuccess) return ctx_cuda(ctx, e, "search_many hits");
+        if (dest.off) {
+            ea.hit_pat = (uint32_t *)ctx->dict_hits.ptr;
+            ea.hit_off = (unsigned long long *)((uint8_t *)ctx->dict_hits.ptr + off_at);
+        } else {
+            ea.hits = (uint2 *)ctx->dict_hits.ptr;
+        }
     }
-    e = launch_dict_emit(ea, st);
-    if (e == cudaSuccess && !d_hits) e = cudaMemcpyAsync(host_hits, ea.hits, k * 8, cudaMemcpyDeviceToHost, st);
+    {
+        GpuPass pass(ctx, "dictionary: emit");
+        e = launch_dict_emit(ea, st);
+    }
+    if (e == cudaSuccess && (dest.host || dest.pair_on_host)) {
+        GpuPass pass(ctx, "download");
+        if (dest.pair_on_host) {
+            e = cudaMemcpyAsync(dest.pat, ea.hit_pat, k * 4, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(dest.off, ea.hit_off, k * 8, cudaMemcpyDeviceToHost, st);
+        } else {
+            e = cudaMemcpyAsync(dest.host, ea.hits, k * 8, cudaMemcpyDeviceToHost, st);
+        }
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    prof_mark(ctx, "dictionary: emit hits");
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "search_many emit");
     return OL_OK;
 }
@@ -517,7 +550,9 @@ extern "C" ol_status ol_search_many(ol_ctx *ctx, const ol_doc *d, const ol_patse
     if (set->ctx != ctx) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "pattern set belongs to another context");
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
-    return many_run(ctx, d, set, max_hits, 0, counts, total_hits, hits, nullptr, nullptr, nullptr, 0);
+    HitDest dest;
+    dest.host = hits;
+    return many_run(ctx, d, set, max_hits, 0, counts, total_hits, dest, nullptr, nullptr, 0);
 }
 
 extern "C" ol_status ol_search_many_device(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits,
@@ -527,7 +562,38 @@ extern "C" ol_status ol_search_many_device(ol_ctx *ctx, const ol_doc *d, const o
     if (set->ctx != ctx) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "pattern set belongs to another context");
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
-    return many_run(ctx, d, set, max_hits, heavy_min_hits, counts, total_hits, nullptr, d_hits, nullptr, nullptr, 0);
+    HitDest dest;
+    dest.dev = d_hits;
+    return many_run(ctx, d, set, max_hits, heavy_min_hits, counts, total_hits, dest, nullptr, nullptr, 0);
+}
+
+extern "C" ol_status ol_search_many_u64(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits,
+                                        uint32_t *counts, uint64_t *total_hits, uint32_t *patterns, uint64_t *offsets) {
+    if (!ctx || !d || !set || !counts || !total_hits || (max_hits && (!patterns || !offsets))) return OL_ERR_INVALID_ARG;
+    if (set->ctx != ctx) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "pattern set belongs to another context");
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    HitDest dest;
+    dest.pat = patterns;
+    dest.off = offsets;
+    dest.pair_on_host = true;
+    return many_run(ctx, d, set, max_hits, 0, counts, total_hits, dest, nullptr, nullptr, 0);
+}
+
+extern "C" ol_status ol_search_many_device_u64(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits,
+                                               uint32_t heavy_min_hits, uint32_t *counts, uint64_t *total_hits,
+                                               uint32_t *d_patterns, uint64_t *d_offsets) {
+    if (!ctx || !d || !set || !counts || !total_hits || (max_hits && (!d_patterns || !d_offsets)))
+        return OL_ERR_INVALID_ARG;
+    if (((uintptr_t)d_offsets & 7) || ((uintptr_t)d_patterns & 3))
+        return ctx_fail(ctx, OL_ERR_INVALID_ARG, "d_offsets must be 8-byte and d_patterns 4-byte aligned");
+    if (set->ctx != ctx) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "pattern set belongs to another context");
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    HitDest dest;
+    dest.pat = d_patterns;
+    dest.off = d_offsets;
+    return many_run(ctx, d, set, max_hits, heavy_min_hits, counts, total_hits, dest, nullptr, nullptr, 0);
 }
 
 extern "C" ol_status ol_dict_stats(ol_ctx *ctx, uint64_t *out) {

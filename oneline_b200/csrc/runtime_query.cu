@@ -44,12 +44,20 @@ ol_status run_query(ol_ctx *ctx, const ol_doc *d, const FlatNode *nodes, uint32_
     a.total = w + 2 * ld;
     a.out = w + 2 * ld + 4;
     a.max_out = max_matches;
-    e = launch_query(a, st);
+    {
+        GpuPass pass(ctx, "query");
+        e = launch_query(a, st);
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(total, a.total, 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    prof_mark(ctx, "query: wait for the count");
     const uint32_t k = std::min(*total, max_matches);
-    if (e == cudaSuccess && k) e = cudaMemcpyAsync(out, a.out, (size_t)k * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && k) {
+        GpuPass pass(ctx, "download");
+        e = cudaMemcpyAsync(out, a.out, (size_t)k * 4, cudaMemcpyDeviceToHost, st);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    prof_mark(ctx, "query: download matches");
     return ctx_cuda(ctx, e, "query");
 }
 

@@ -68,6 +68,7 @@ cudaError_t enqueue_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *pa
 cudaError_t ol::launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *hpats, const uint8_t *const *dpats,
                              const uint32_t *lens, uint32_t n, const uint32_t *max_out, uint32_t *d_totals,
                              uint32_t *const *d_outs) {
+    GpuPass pass(ctx, "search");
     cudaStream_t st = ctx->stream;
     uint32_t n_tiles = (uint32_t)((d->text_len + kSearchTile - 1) / kSearchTile);
     const size_t col_words = (size_t)scan_ld(n_tiles) * kSearchMaxPatterns;  // counts, then bases
@@ -149,15 +150,20 @@ ol_status search_multi_host(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *
         uint32_t tot_h[64];
         if (e == cudaSuccess) e = cudaMemcpyAsync(tot_h, d_totals, cn * 4, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        prof_mark(ctx, "search: wait for totals");
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "search");
-        for (uint32_t j = 0; j < cn; j++) {
-            uint32_t i = idx[c + j];
-            totals[i] = tot_h[j];
-            uint32_t k = std::min(tot_h[j], max_matches[i]);
-            if (k > 0 && (e = cudaMemcpyAsync(outs[i], o2[c + j], (size_t)k * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-                return ctx_cuda(ctx, e, "search download");
+        {
+            GpuPass pass(ctx, "download");
+            for (uint32_t j = 0; j < cn; j++) {
+                uint32_t i = idx[c + j];
+                totals[i] = tot_h[j];
+                uint32_t k = std::min(tot_h[j], max_matches[i]);
+                if (k > 0 && (e = cudaMemcpyAsync(outs[i], o2[c + j], (size_t)k * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+                    return ctx_cuda(ctx, e, "search download");
+            }
         }
         if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx_cuda(ctx, e, "search download");
+        prof_mark(ctx, "search: download matches");
     }
     return OL_OK;
 }

@@ -102,12 +102,17 @@ ol_status build(ol_ctx *ctx, const ol_doc *d, ol_tree *t, uint32_t flags, bool w
     ol_status s = tree_alloc(ctx, t, L);
     if (s != OL_OK) return s;
     t->deep = deep;
-    cudaError_t e = deep ? enqueue_tree_deep(ctx, d, t) : enqueue_tree_fast(ctx, d, t);
+    cudaError_t e;
+    {
+        GpuPass pass(ctx, "tree");
+        e = deep ? enqueue_tree_deep(ctx, d, t) : enqueue_tree_fast(ctx, d, t);
+    }
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "tree");
     if (!wait) return OL_OK;
     uint32_t err = 0;
     e = cudaMemcpyAsync(&ctx->host_counters->error, &d->stats->error, 4, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    prof_mark(ctx, "tree: wait for links");
     if (e != cudaSuccess) return ctx_cuda(ctx, e, "tree");
     err = ctx->host_counters->error;
     if (err & OL_DEVERR_DEEP) return ctx_fail(ctx, OL_ERR_CUDA, "tree: depth above the fast path reached the kernels");

@@ -113,7 +113,7 @@ extern "C" ol_status ol_autotune(ol_ctx *ctx, const ol_doc *d, const ol_patset *
         std::vector<uint32_t> counts(ol_patset_len(set));
         uint64_t total = 0;
         auto run = [&]() {
-            return many_run(ctx, d, set, 0, 0, counts.data(), &total, nullptr, nullptr, nullptr, nullptr, 0) == OL_OK;
+            return many_run(ctx, d, set, 0, 0, counts.data(), &total, HitDest{}, nullptr, nullptr, 0) == OL_OK;
         };
         double best_t = 1e30;
         for (uint32_t slice : {256u, 512u, 1024u})

@@ -194,8 +194,9 @@ void run_search(ol_server *s, ol_ctx *ctx, unsigned long long *d_digest, ol_hit 
         st = ol_patset_compile(ctx, e.doc, p.data(), lens.data(), (uint32_t)p.size(), &set);
         std::vector<uint32_t> counts(p.size());
         uint64_t total = 0;
-        if (st == OL_OK)
-            st = many_run(ctx, e.doc, set, s->max_hits, 0, counts.data(), &total, nullptr, d_hits, nullptr, nullptr, 0);
+        HitDest dest;
+        dest.dev = d_hits;
+        if (st == OL_OK) st = many_run(ctx, e.doc, set, s->max_hits, 0, counts.data(), &total, dest, nullptr, nullptr, 0);
         if (st == OL_OK) {
             const uint64_t k = std::min<uint64_t>(total, s->max_hits);
             unsigned long long h = 0;

@@ -11,6 +11,8 @@ Method names, argument meaning and error behaviour follow the reference:
                                                         document.rs:94-127, tree.rs:292-313, query.rs:10-19, 228-329
 * ``GpuParser.compile_patterns`` / ``search_many`` / ``GpuPatternSet`` / ``ManyResult``
                                                         many.rs:14-18, 76-94, 139-176, 391-399
+* ``GpuParser.profile_*`` / ``Profile``                 timing.rs:109-124, document.rs:136-157, search.rs:143-173,
+                                                        many.rs:401-410, tree.rs:69-82, query.rs:275
 * limits ``MAX_PATTERN_LEN``, ``MAX_TREE_DEPTH``, ``MAX_GPU_INPUT_LEN``  lib.rs:66, tree.rs:12, util.rs:8
 
 Errors are raised as ``OnelineError`` (the reference returns ``anyhow::Error``);
@@ -60,6 +62,37 @@ def _check_len(n: int) -> None:
     if n > MAX_GPU_INPUT_LEN:
         raise OnelineError(2, f"input is {n} bytes; the GPU path addresses at most {MAX_GPU_INPUT_LEN} bytes "
                               "(32-bit offsets)")
+
+
+class _ProfileStep(ctypes.Structure):
+    _fields_ = [("label", ctypes.c_char * 40), ("ns", ctypes.c_uint64)]
+
+
+class _Profile(ctypes.Structure):
+    """ol_profile (include/oneline_cuda.h)."""
+
+    _fields_ = [("wall_ns", ctypes.c_uint64), ("gpu_total_ns", ctypes.c_uint64), ("n_host_steps", ctypes.c_uint32),
+                ("n_gpu_passes", ctypes.c_uint32), ("host_steps", _ProfileStep * 32), ("gpu_passes", _ProfileStep * 32)]
+
+
+@dataclass
+class Profile:
+    """Where the time of one run went (timing.rs:109-124): host wall clock, the
+    host steps in order (time since the previous step) and the GPU passes with
+    their device time (CUDA events), all in seconds."""
+
+    wall: float
+    host_steps: list
+    gpu_passes: list
+
+    def gpu_total(self) -> float:
+        return sum(d for _, d in self.gpu_passes)
+
+    @staticmethod
+    def _from(raw: _Profile) -> "Profile":
+        steps = [(raw.host_steps[i].label.decode(), raw.host_steps[i].ns / 1e9) for i in range(raw.n_host_steps)]
+        passes = [(raw.gpu_passes[i].label.decode(), raw.gpu_passes[i].ns / 1e9) for i in range(raw.n_gpu_passes)]
+        return Profile(raw.wall_ns / 1e9, steps, passes)
 
 
 @dataclass
@@ -574,6 +607,31 @@ class GpuParser:
                                                 d_hits), self._ctx)
         return counts, int(total.value)
 
+    def search_many_u64(self, doc: GpuDocument, pattern_set: GpuPatternSet, max_hits: int) -> tuple:
+        """``search_many`` in the (pattern id u32, byte offset u64) form: returns
+        (counts, total_hits, patterns u32[k], offsets u64[k]), k = min(total, max_hits)."""
+        if max_hits < 0:
+            raise OnelineError(1, "max_hits must not be negative")
+        counts = np.zeros(len(pattern_set), np.uint32)
+        total = ctypes.c_uint64()
+        pats = np.zeros(max(int(max_hits), 1), np.uint32)
+        offs = np.zeros(max(int(max_hits), 1), np.uint64)
+        check(_lib.load().ol_search_many_u64(self._ctx, doc.handle, pattern_set.handle, int(max_hits),
+                                             counts.ctypes.data, ctypes.byref(total), pats.ctypes.data,
+                                             offs.ctypes.data), self._ctx)
+        k = min(int(total.value), int(max_hits))
+        return counts, int(total.value), pats[:k].copy(), offs[:k].copy()
+
+    def search_many_device_u64(self, doc: GpuDocument, pattern_set: GpuPatternSet, d_patterns: int, d_offsets: int,
+                               max_hits: int, *, heavy_min_hits: int = 0) -> tuple[np.ndarray, int]:
+        """``search_many_u64`` with the two arrays in device memory; returns (counts, total_hits)."""
+        counts = np.zeros(len(pattern_set), np.uint32)
+        total = ctypes.c_uint64()
+        check(_lib.load().ol_search_many_device_u64(self._ctx, doc.handle, pattern_set.handle, int(max_hits),
+                                                    int(heavy_min_hits), counts.ctypes.data, ctypes.byref(total),
+                                                    d_patterns, d_offsets), self._ctx)
+        return counts, int(total.value)
+
     # -------------------------------------------------------------- batches
 
     def upload_batch(self, docs) -> GpuBatch:
@@ -670,6 +728,47 @@ class GpuParser:
     def tuning_load(self, path: str) -> dict:
         check(_lib.load().ol_tuning_load(self._ctx, path.encode()), self._ctx)
         return self.tuning
+
+    # ------------------------------------------------------------ profiling
+
+    def _profiled(self, fn, *args, **kw):
+        """(fn's result, Profile) with the context's profile open around fn."""
+        L = _lib.load()
+        check(L.ol_profile_begin(self._ctx), self._ctx)
+        raw = _Profile()
+        try:
+            out = fn(*args, **kw)
+        finally:
+            st = L.ol_profile_end(self._ctx, ctypes.byref(raw))
+        check(st, self._ctx)
+        return out, Profile._from(raw)
+
+    def profile_upload(self, text) -> tuple[GpuDocument, Profile]:
+        """``upload``, with a breakdown of where the time went (waits for the parse)."""
+        return self._profiled(self.upload, text)
+
+    def profile_query_document(self, doc: GpuDocument, kind=None, depth=None, max_matches: int = 1 << 20) -> Profile:
+        return self._profiled(self.query_document, doc, kind, depth, max_matches)[1]
+
+    def profile_search_document(self, doc: GpuDocument, pattern: bytes, max_matches: int) -> Profile:
+        return self._profiled(self.search_document, doc, pattern, max_matches)[1]
+
+    def profile_search_raw(self, text, pattern: bytes, max_matches: int) -> Profile:
+        return self._profiled(self.search_raw, text, pattern, max_matches)[1]
+
+    def profile_search_many(self, doc: GpuDocument, pattern_set: "GpuPatternSet", max_hits: int) -> Profile:
+        return self._profiled(self.search_many, doc, pattern_set, max_hits)[1]
+
+    def profile_build_tree_reusing(self, doc: GpuDocument, previous: "GpuTree | None") -> tuple["GpuTree", Profile]:
+        return self._profiled(self.build_tree_reusing, doc, previous)
+
+    def profile_build_tree(self, doc: GpuDocument) -> Profile:
+        tree, prof = self.profile_build_tree_reusing(doc, None)
+        tree.free()
+        return prof
+
+    def profile_query_raw(self, text, kind=None, depth=None, max_matches: int = 1 << 20) -> Profile:
+        return self._profiled(self.query_raw, text, kind, depth, max_matches)[1]
 
     def dict_stats(self) -> dict:
         """Work of the last dictionary search: positions walked, trie nodes visited,

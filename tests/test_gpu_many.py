@@ -166,3 +166,26 @@ def test_injected_wait_timeout_is_reported_and_leaves_the_context_usable(parser)
         parser.search_many(doc, ps, 1 << 20)
     assert ei.value.status == 7 and "bounded wait" in str(ei.value), ei.value
     assert_many(parser, text, pats, what="after the injected timeout")
+
+
+def test_u64_offset_form_equals_the_manyhit_form(parser):
+    """The (pattern u32, offset u64) hit form: the same hits as ManyHit, host and
+    device arrays, truncated and whole."""
+    import torch
+
+    text = datagen.corpus(3 << 20, 22).tobytes()
+    pats = datagen.patterns_dictionary(np.frombuffer(text, np.uint8), 22, n=500) + [b"||||", b"||||"]
+    counts, hp, ho = oracle.find_many(text, pats)
+    doc = parser.upload(text)
+    ps = parser.compile_patterns(doc, pats)
+    total = len(hp)
+    for cap in (total, total // 3):
+        c, t, pp, oo = parser.search_many_u64(doc, ps, cap)
+        assert t == total and np.array_equal(c.astype(np.uint64), counts)
+        assert oo.dtype == np.uint64 and np.array_equal(pp, hp[:cap]) and np.array_equal(oo, ho[:cap].astype(np.uint64))
+    d_p = torch.full((total,), -1, dtype=torch.int32, device="cuda")
+    d_o = torch.full((total,), -1, dtype=torch.int64, device="cuda")
+    c, t = parser.search_many_device_u64(doc, ps, d_p.data_ptr(), d_o.data_ptr(), total, heavy_min_hits=1)
+    assert t == total
+    assert np.array_equal(d_p.cpu().numpy().view(np.uint32), hp)
+    assert np.array_equal(d_o.cpu().numpy().view(np.uint64), ho.astype(np.uint64))
