@@ -331,15 +331,22 @@ ol_status ol_batch_search_many(ol_ctx *ctx, const ol_batch *batch, const ol_pats
 
 /* ---- serving. No counterpart in the reference (one blocking call per
  *      document). A server owns `workers` threads, each with its own context
- *      and stream: queued requests start as soon as a worker frees up and their
- *      kernels overlap on the device. Parsed documents (text, line arrays, tree
- *      links) stay resident in a store of at most store_budget bytes: the least
- *      recently used idle documents are evicted to make room, and a document
- *      that does not fit beside the ones in use is refused (OL_ERR_ADMISSION).
- *      A search names a resident document (OL_ERR_NOT_FOUND once evicted) and
- *      searches it for 1..OL_MAX_DICT_PATTERNS set patterns; each worker keeps
- *      up to max_hits hits in device memory. Results carry a digest of the
- *      outputs, computed on the device, to compare runs. */
+ *      and stream. Continuous batching: a worker that frees up takes every
+ *      request queued at that moment and serves them as one step: parse
+ *      requests are admitted against the store budget before any upload
+ *      (counting the reservations of requests in flight; refused with
+ *      OL_ERR_ADMISSION when they cannot fit), then uploaded, parsed and
+ *      linked as one batch; search requests on the same document share one
+ *      dictionary pass. Steps of different workers overlap on the device.
+ *      Parsed documents (text, line arrays, tree links) stay resident in a
+ *      store of at most store_budget bytes: the least recently used idle
+ *      documents are evicted to make room. A search names a resident document
+ *      (OL_ERR_NOT_FOUND once evicted) and searches it for
+ *      1..OL_MAX_DICT_PATTERNS set patterns of OL_MIN_SET_PATTERN_LEN..
+ *      OL_MAX_SET_PATTERN_LEN bytes, keeping up to max_hits hits. A request
+ *      completes once its results are in host memory (the caller's buffers
+ *      when given); each result carries a digest of its outputs, to compare a
+ *      request served in a busy mix with the same request alone. */
 typedef struct ol_server ol_server;
 typedef struct ol_request_result {
     uint64_t id;
@@ -354,16 +361,50 @@ typedef struct ol_request_result {
     uint64_t submit_ns, start_ns, end_ns;  /* steady clock */
 } ol_request_result;
 ol_status ol_server_create(int32_t device, uint32_t workers, uint64_t store_budget, uint64_t max_hits, ol_server **out);
+/* Same, with flags. OL_SERVER_NO_COALESCE: one request per step (the plain
+ * per-request form, for comparison). */
+#define OL_SERVER_NO_COALESCE 1u
+ol_status ol_server_create_ex(int32_t device, uint32_t workers, uint64_t store_budget, uint64_t max_hits,
+                              uint32_t flags, ol_server **out);
+/* Where a request's results go (host memory that must stay valid until the
+ * request completes). Parse: every array holds `cap` entries and is written
+ * when the document's line count fits (any pointer may be NULL). Search:
+ * counts[i] for the request's pattern i, and its first min(total, max_hits)
+ * hits, pattern = index in the request's list (either pointer may be NULL;
+ * max_hits also caps what the digest covers). */
+typedef struct ol_parse_dest {
+    uint64_t cap;
+    uint32_t *offsets;
+    uint8_t *kinds;
+    uint32_t *parent, *subtree_end, *first_child, *next_sibling;
+} ol_parse_dest;
+typedef struct ol_search_dest {
+    uint64_t max_hits;
+    uint32_t *counts;
+    ol_hit *hits;
+} ol_search_dest;
 /* Finishes the queued requests, then frees every resident document. */
 void ol_server_destroy(ol_server *server);
 /* The text must stay valid until the request completes. */
 ol_status ol_server_submit_parse(ol_server *server, const uint8_t *text, uint64_t len, uint64_t *request_id);
 ol_status ol_server_submit_search(ol_server *server, uint64_t doc_id, const uint8_t *const *patterns,
                                   const uint32_t *lens, uint32_t n, uint64_t *request_id);
+/* The same with the results copied to `dest` (may be NULL). */
+ol_status ol_server_submit_parse_to(ol_server *server, const uint8_t *text, uint64_t len, const ol_parse_dest *dest,
+                                    uint64_t *request_id);
+ol_status ol_server_submit_search_to(ol_server *server, uint64_t doc_id, const uint8_t *const *patterns,
+                                     const uint32_t *lens, uint32_t n, const ol_search_dest *dest,
+                                     uint64_t *request_id);
 /* Blocks until the request is done and returns its result (once). */
 ol_status ol_server_wait(ol_server *server, uint64_t request_id, ol_request_result *out);
 ol_status ol_server_stats(ol_server *server, uint64_t *resident_docs, uint64_t *resident_bytes, uint64_t *evictions,
                           uint64_t *refusals);
+/* While paused, workers finish their current step and take no new request;
+ * requests still queue (for draining, and to hand a set of requests to one
+ * step). Destroying a paused server serves what is queued first. */
+ol_status ol_server_pause(ol_server *server, uint32_t paused);
+/* Steps served, requests served, and the most requests one step took. */
+ol_status ol_server_steps(ol_server *server, uint64_t *steps, uint64_t *requests, uint64_t *largest_step);
 
 /* ---- substring search that allocates nothing. No counterpart in the
  *      reference: an addition for callers that cannot call cudaMalloc, such as a

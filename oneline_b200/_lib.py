@@ -96,6 +96,11 @@ SIGNATURES: dict[str, tuple] = {
     "ol_batch_read_doc": (_S, [_P, _P, _U32, _P, _P, _P, _P, _P, _P, _U64]),
     "ol_batch_search_many": (_S, [_P, _P, _P, _U64, _U32, _P, _U64P, _P]),
     "ol_server_create": (_S, [_I32, _U32, _U64, _U64, _PP]),
+    "ol_server_create_ex": (_S, [_I32, _U32, _U64, _U64, _U32, _PP]),
+    "ol_server_submit_parse_to": (_S, [_P, _U8P, _U64, _P, _U64P]),
+    "ol_server_submit_search_to": (_S, [_P, _U64, _P, _P, _U32, _P, _U64P]),
+    "ol_server_pause": (_S, [_P, _U32]),
+    "ol_server_steps": (_S, [_P, _U64P, _U64P, _U64P]),
     "ol_server_destroy": (None, [_P]),
     "ol_server_submit_parse": (_S, [_P, _U8P, _U64, _U64P]),
     "ol_server_submit_search": (_S, [_P, _U64, _P, _P, _U32, _U64P]),

@@ -8,6 +8,8 @@
 // those of core links.rs:52-82 and simd search.rs:259-282.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "ol_common.cuh"
 #include "ol_kernels.h"
 
@@ -78,6 +80,61 @@ __global__ void batch_tree_fixup_kernel(const uint32_t *__restrict__ line_start,
     subtree_end[j] = e;
     first_child[j] = (f != NONE && f < le) ? f : NONE;
     next_sibling[j] = ns;
+}
+
+// Documents of a parsed, linked batch copied into their own resident buffers,
+// all in one launch. Work item k of document i covers its text bytes
+// [k * 4096, +4096) and its lines [k * 1024, +1024); offsets lose the
+// document's first byte, tree links its first line (NONE stays NONE), and
+// max_depth[i] receives the document's deepest non-blank line (from depth8,
+// so 255 stands for 255 or more).
+constexpr uint32_t kSplitBytes = 4096, kSplitLines = 1024;
+
+__global__ void batch_split_kernel(const BatchSplitDoc *__restrict__ docs, const uint32_t *__restrict__ item_start,
+                                   uint32_t n, BatchSplitSrc src, uint32_t *__restrict__ max_depth) {
+    const uint32_t item = blockIdx.x;
+    uint32_t lo = 0, hi = n;  // the last document i with item_start[i] <= item
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(item_start + mid) <= item)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    const BatchSplitDoc d = docs[lo];
+    const uint32_t k = item - __ldg(item_start + lo);
+    const uint64_t b0 = (uint64_t)k * kSplitBytes;
+    for (uint64_t j = b0 + threadIdx.x; j < d.text_len && j < b0 + kSplitBytes; j += blockDim.x)
+        d.text[j] = src.text[d.text_start + j];
+    const uint32_t l0 = k * kSplitLines;
+    uint32_t deepest = 0;
+    for (uint32_t j = l0 + threadIdx.x; j < d.lines && j < l0 + kSplitLines; j += blockDim.x) {
+        const uint32_t g = d.first_line + j;
+        const uint8_t kind = src.kinds[g], depth = src.depth8[g];
+        d.offsets[j] = src.offsets[g] - (uint32_t)d.text_start;
+        d.kinds[j] = kind;
+        d.depth8[j] = depth;
+        if (kind != KIND_BLANK) deepest = max(deepest, (uint32_t)depth);
+        auto rebase = [&](uint32_t v) { return v == NONE ? NONE : v - d.first_line; };
+        d.parent[j] = rebase(src.parent[g]);
+        d.subtree_end[j] = rebase(src.subtree_end[g]);
+        d.first_child[j] = rebase(src.first_child[g]);
+        d.next_sibling[j] = rebase(src.next_sibling[g]);
+    }
+    for (int o = 16; o > 0; o >>= 1) deepest = max(deepest, __shfl_xor_sync(0xFFFFFFFFu, deepest, o));
+    if ((threadIdx.x & 31) == 0 && deepest) atomicMax(max_depth + lo, deepest);
+}
+
+uint32_t batch_split_items(uint64_t text_len, uint32_t lines) {
+    const uint64_t a = (text_len + kSplitBytes - 1) / kSplitBytes, b = (lines + kSplitLines - 1) / kSplitLines;
+    return (uint32_t)std::max<uint64_t>(std::max(a, b), 1);
+}
+
+cudaError_t launch_batch_split(const BatchSplitDoc *docs, const uint32_t *item_start, uint32_t n, uint32_t items,
+                               const BatchSplitSrc &src, uint32_t *max_depth, cudaStream_t st) {
+    if (n == 0 || items == 0) return cudaSuccess;
+    batch_split_kernel<<<items, 256, 0, st>>>(docs, item_start, n, src, max_depth); OL_LAUNCHED();
+    return cudaGetLastError();
 }
 
 cudaError_t launch_batch_line_starts(const uint32_t *offsets, uint32_t L, const unsigned long long *seg_start, uint32_t n,

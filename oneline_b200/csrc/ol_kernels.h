@@ -293,4 +293,26 @@ cudaError_t launch_batch_tree_fixup(const uint32_t *line_start, uint32_t n, uint
                                     uint32_t *next_sibling, cudaStream_t st);
 cudaError_t launch_dict_emit(const DictEmitArgs &a, cudaStream_t st);
 
+// One document of a batch and the buffers it is copied into (batch_split).
+struct BatchSplitDoc {
+    uint64_t text_start, text_len;  // bytes of the batch text
+    uint32_t first_line, lines;     // lines of the batch
+    uint8_t *text;
+    uint32_t *offsets;
+    uint8_t *kinds, *depth8;
+    uint32_t *parent, *subtree_end, *first_child, *next_sibling;
+};
+struct BatchSplitSrc {
+    const uint8_t *text;
+    const uint32_t *offsets;
+    const uint8_t *kinds, *depth8;
+    const uint32_t *parent, *subtree_end, *first_child, *next_sibling;
+};
+// Work items of a document (batch_split_kernel: 4096 bytes and 1024 lines each).
+uint32_t batch_split_items(uint64_t text_len, uint32_t lines);
+// item_start[i]: the first work item of document i (a prefix sum of
+// batch_split_items); items: their total.
+cudaError_t launch_batch_split(const BatchSplitDoc *docs, const uint32_t *item_start, uint32_t n, uint32_t items,
+                               const BatchSplitSrc &src, uint32_t *max_depth, cudaStream_t st);
+
 }  // namespace ol

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/oneline_cuda.h"
 #include "ol_common.cuh"
@@ -128,6 +129,11 @@ struct HitDest {
     uint64_t *off = nullptr;
     bool pair_on_host = false;
 };
+ol_status batch_from_parts(ol_ctx *ctx, const uint8_t *const *parts, const uint64_t *lens, uint32_t n, ol_batch **out);
+ol_status batch_split(ol_ctx *ctx, ol_batch *b, std::vector<ol_doc *> &docs, std::vector<ol_tree *> &trees);
+uint64_t estimate_lines(const uint8_t *host, uint64_t len);
+ol_status alloc_lines(ol_ctx *ctx, ol_doc *d, uint64_t cap_lines);
+ol_status tree_alloc(ol_ctx *ctx, ol_tree *t, uint32_t L);
 ol_status many_run(ol_ctx *ctx, const ol_doc *d, const ol_patset *set, uint64_t max_hits, uint32_t heavy_min_hits,
                    uint32_t *counts, uint64_t *total, const HitDest &dest,
                    const unsigned long long *seg_start, const unsigned long long *seg_end, uint32_t n_seg);

@@ -29,13 +29,11 @@ struct ol_batch {
     uint32_t *d_line_start = nullptr;
 };
 
-extern "C" ol_status ol_batch_upload(ol_ctx *ctx, const uint8_t *data, const uint64_t *doc_offsets, uint32_t n,
-                                     ol_batch **out) {
-    if (!ctx || !out || !doc_offsets || n == 0) return OL_ERR_INVALID_ARG;
+// The batch of documents parts[i][0 .. lens[i]) (host memory), uploaded and
+// parsed (see ol_batch_upload).
+ol_status ol::batch_from_parts(ol_ctx *ctx, const uint8_t *const *parts, const uint64_t *lens, uint32_t n,
+                               ol_batch **out) {
     *out = nullptr;
-    for (uint32_t i = 0; i < n; i++)
-        if (doc_offsets[i + 1] < doc_offsets[i]) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "document offsets must not decrease");
-    if (doc_offsets[n] > doc_offsets[0] && !data) return OL_ERR_INVALID_ARG;
     // Layout: document bytes, then '\n' when the document is non-empty and does
     // not already end in one.
     auto b = new ol_batch();
@@ -45,10 +43,10 @@ extern "C" ol_status ol_batch_upload(ol_ctx *ctx, const uint8_t *data, const uin
     b->len.resize(n);
     uint64_t T = 0;
     for (uint32_t i = 0; i < n; i++) {
-        const uint64_t l = doc_offsets[i + 1] - doc_offsets[i];
+        const uint64_t l = lens[i];
         b->start[i] = T;
         b->len[i] = l;
-        T += l + ((l && data[doc_offsets[i + 1] - 1] != '\n') ? 1 : 0);
+        T += l + ((l && parts[i][l - 1] != '\n') ? 1 : 0);
     }
     if (T > OL_MAX_GPU_INPUT_LEN) {
         delete b;
@@ -96,8 +94,8 @@ extern "C" ol_status ol_batch_upload(ol_ctx *ctx, const uint8_t *data, const uin
     static const uint8_t nl = '\n';
     for (uint32_t i = 0; s == OL_OK && e == cudaSuccess && i < n; i++) {
         const uint64_t l = b->len[i];
-        if (l) e = put(data + doc_offsets[i], l);
-        if (e == cudaSuccess && l && data[doc_offsets[i + 1] - 1] != '\n') e = put(&nl, 1);
+        if (l) e = put(parts[i], l);
+        if (e == cudaSuccess && l && parts[i][l - 1] != '\n') e = put(&nl, 1);
     }
     if (s == OL_OK && e == cudaSuccess) e = flush();
     if (s == OL_OK && e != cudaSuccess) s = ctx_cuda(ctx, e, "batch upload");
@@ -129,6 +127,22 @@ extern "C" ol_status ol_batch_upload(ol_ctx *ctx, const uint8_t *data, const uin
     }
     *out = b;
     return OL_OK;
+}
+
+extern "C" ol_status ol_batch_upload(ol_ctx *ctx, const uint8_t *data, const uint64_t *doc_offsets, uint32_t n,
+                                     ol_batch **out) {
+    if (!ctx || !out || !doc_offsets || n == 0) return OL_ERR_INVALID_ARG;
+    *out = nullptr;
+    for (uint32_t i = 0; i < n; i++)
+        if (doc_offsets[i + 1] < doc_offsets[i]) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "document offsets must not decrease");
+    if (doc_offsets[n] > doc_offsets[0] && !data) return OL_ERR_INVALID_ARG;
+    std::vector<const uint8_t *> parts(n);
+    std::vector<uint64_t> lens(n);
+    for (uint32_t i = 0; i < n; i++) {
+        parts[i] = data ? data + doc_offsets[i] : nullptr;
+        lens[i] = doc_offsets[i + 1] - doc_offsets[i];
+    }
+    return batch_from_parts(ctx, parts.data(), lens.data(), n, out);
 }
 
 extern "C" void ol_batch_free(ol_batch *b) {
@@ -236,4 +250,98 @@ extern "C" ol_status ol_batch_search_many(ol_ctx *ctx, const ol_batch *b, const 
     dest.dev = d_hits;
     return many_run(ctx, b->doc, set, max_hits, heavy_min_hits, counts, total_hits, dest, b->seg_start,
                     b->seg_end, b->n);
+}
+
+// Splits a parsed batch whose trees are built into its documents: each gets
+// its own resident document and tree, equal to what ol_doc_upload and
+// ol_tree_build of that document alone give, with one copy launch for all of
+// them. docs[i] / trees[i] are new handles on ctx (an empty document gets a
+// document without lines and a tree of 0 lines).
+ol_status ol::batch_split(ol_ctx *ctx, ol_batch *b, std::vector<ol_doc *> &docs, std::vector<ol_tree *> &trees) {
+    if (!b->tree) return ctx_fail(ctx, OL_ERR_INVALID_ARG, "batch_split: the batch's trees are not built");
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const uint32_t n = b->n;
+    docs.assign(n, nullptr);
+    trees.assign(n, nullptr);
+    std::vector<BatchSplitDoc> table;
+    std::vector<uint32_t> item_start, which;
+    uint32_t items = 0;
+    ol_status s = OL_OK;
+    cudaError_t e = cudaSuccess;
+    for (uint32_t i = 0; i < n && s == OL_OK; i++) {
+        uint64_t ls, lc;
+        ol_batch_doc_info(b, i, nullptr, nullptr, &ls, &lc);
+        s = new_doc(ctx, b->len[i], &docs[i]);
+        if (s != OL_OK) break;
+        trees[i] = new ol_tree();
+        trees[i]->ctx = ctx;
+        if (b->len[i] == 0) continue;
+        ol_doc *d = docs[i];
+        s = alloc_lines(ctx, d, lc);
+        if (s == OL_OK) s = tree_alloc(ctx, trees[i], (uint32_t)lc);
+        if (s != OL_OK) break;
+        if ((e = cudaMemsetAsync(d->stats, 0, sizeof(DocStats), st)) != cudaSuccess) break;
+        d->line_count = (uint32_t)lc;
+        trees[i]->line_count = (uint32_t)lc;
+        BatchSplitDoc x;
+        x.text_start = b->start[i];
+        x.text_len = b->len[i];
+        x.first_line = (uint32_t)ls;
+        x.lines = (uint32_t)lc;
+        x.text = d->text;
+        x.offsets = d->offsets;
+        x.kinds = d->kinds;
+        x.depth8 = d->depth8;
+        x.parent = (uint32_t *)trees[i]->parent_buf.ptr;
+        x.subtree_end = (uint32_t *)trees[i]->end_buf.ptr;
+        x.first_child = (uint32_t *)trees[i]->fc_buf.ptr;
+        x.next_sibling = (uint32_t *)trees[i]->ns_buf.ptr;
+        table.push_back(x);
+        item_start.push_back(items);
+        which.push_back(i);
+        items += batch_split_items(x.text_len, x.lines);
+    }
+    const uint32_t m = (uint32_t)table.size();
+    std::vector<uint32_t> depth(m, 0);
+    if (s == OL_OK && e == cudaSuccess && m) {
+        const size_t t_bytes = (size_t)m * sizeof(BatchSplitDoc), i_at = (t_bytes + 15) & ~size_t(15);
+        const size_t d_at = (i_at + (size_t)m * 4 + 15) & ~size_t(15);
+        e = ctx->scratch_b.reserve(d_at + (size_t)m * 4, st);
+        uint8_t *base = (uint8_t *)ctx->scratch_b.ptr;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(base, table.data(), t_bytes, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(base + i_at, item_start.data(), (size_t)m * 4, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(base + d_at, 0, (size_t)m * 4, st);
+        BatchSplitSrc src;
+        src.text = b->doc->text;
+        src.offsets = b->doc->offsets;
+        src.kinds = b->doc->kinds;
+        src.depth8 = b->doc->depth8;
+        src.parent = (const uint32_t *)b->tree->parent_buf.ptr;
+        src.subtree_end = (const uint32_t *)b->tree->end_buf.ptr;
+        src.first_child = (const uint32_t *)b->tree->fc_buf.ptr;
+        src.next_sibling = (const uint32_t *)b->tree->ns_buf.ptr;
+        if (e == cudaSuccess) {
+            GpuPass pass(ctx, "batch: split into documents");
+            e = launch_batch_split((const BatchSplitDoc *)base, (const uint32_t *)(base + i_at), m, items, src,
+                                   (uint32_t *)(base + d_at), st);
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(depth.data(), base + d_at, (size_t)m * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (s == OL_OK && e != cudaSuccess) s = ctx_cuda(ctx, e, "batch split");
+    if (s != OL_OK) {
+        for (auto &t : trees) ol_tree_free(t);
+        for (auto &d : docs) ol_doc_free(d);
+        docs.clear();
+        trees.clear();
+        return s;
+    }
+    for (uint32_t k = 0; k < m; k++) {
+        const uint32_t i = which[k];
+        docs[i]->max_depth = depth[k];
+        trees[i]->deep = depth[k] >= kTreeLevels;
+    }
+    return OL_OK;
 }

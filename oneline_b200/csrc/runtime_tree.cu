@@ -10,9 +10,7 @@
 
 using namespace ol;
 
-namespace {
-
-ol_status tree_alloc(ol_ctx *ctx, ol_tree *t, uint32_t L) {
+ol_status ol::tree_alloc(ol_ctx *ctx, ol_tree *t, uint32_t L) {
     cudaStream_t st = ctx->stream;
     uint32_t cap = round_lines(std::max<uint32_t>(L, 1));
     if (t->capacity >= cap && t->parent_buf.ptr) return OL_OK;
@@ -28,6 +26,8 @@ ol_status tree_alloc(ol_ctx *ctx, ol_tree *t, uint32_t L) {
     t->capacity = cap;
     return OL_OK;
 }
+
+namespace {
 
 // Enqueues the fast (depth < 32) tree kernels.
 cudaError_t enqueue_tree_fast(ol_ctx *ctx, const ol_doc *d, ol_tree *t) {

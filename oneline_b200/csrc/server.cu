@@ -1,25 +1,38 @@
 // A serving loop for parse and search requests of mixed sizes (no reference
 // counterpart: the reference exposes one blocking call per document,
 // crates/oneline-gpu/src/parser.rs). Requests are queued as they arrive and
-// taken by worker threads, each with its own context and CUDA stream, so
-// requests that arrive while others run are admitted as soon as a worker frees
-// up and their kernels overlap on the device. Parsed documents (text, line
-// arrays, tree links) stay resident in a store bounded by an HBM budget: a new
-// document evicts the least recently used idle ones, and is refused
-// (OL_ERR_ADMISSION) when the documents in use leave no room. Search requests
-// name a resident document and never upload text again.
+// taken by worker threads, each with its own context and CUDA stream.
 //
-// Every result carries a digest of its outputs computed on the device (offsets,
-// kinds and the four tree arrays of a parse; counts and hits of a search), so a
-// result computed in a busy server can be compared with the same request run
-// alone.
+// Continuous batching: a worker that frees up takes every request queued at
+// that moment (up to a step's limits) and serves them together:
+//   * admission first: each parse request reserves its estimated resident
+//     bytes against the store budget, counting the reservations of requests
+//     still in flight on other workers; least recently used idle documents
+//     are evicted to make room, and a request that cannot fit is refused
+//     (OL_ERR_ADMISSION) before any upload;
+//   * the admitted parse requests are uploaded, parsed and linked as one batch
+//     (one pinned-ring upload, one parse, one tree build for all of them),
+//     then split into resident documents with one copy launch;
+//   * search requests on the same resident document are merged into one
+//     pattern set and one dictionary pass, and each request gets its own slice
+//     of the (pattern, offset)-ordered hits.
+// Workers run steps concurrently, so requests that arrive while others are on
+// the GPU start on the next free worker and their kernels overlap on the
+// device. Results (offsets, kinds and the four tree arrays of a parse; counts
+// and hits of a search) are downloaded into host memory, and into the caller's
+// buffers when given, before the request completes, so the reported latency
+// includes the download. Every result carries a digest of its outputs,
+// computed on the host from the downloaded arrays, to compare a request served
+// in a busy mix with the same request alone.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -32,10 +45,53 @@ using namespace ol;
 
 namespace {
 
+constexpr uint32_t kStepMaxRequests = 256;             // requests one step takes at most
+constexpr uint64_t kStepMaxParseBytes = 256ull << 20;  // parse text one step takes at most
+constexpr uint64_t kStagingBytes = 64ull << 20;        // pinned download staging per worker (grown on demand)
+constexpr uint64_t kStagingMaxBytes = 2ull << 30;
+
 uint64_t now_ns() {
     return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
                std::chrono::steady_clock::now().time_since_epoch())
         .count();
+}
+
+// The digest of one array: the sum (mod 2^64) over i of
+// splitmix64(seed << 56 ^ i << 24 ^ a[i] * 0x9E3779B97F4A7C15), a sum of
+// per-element hashes, so two arrays that differ in one element or in order
+// differ in digest with overwhelming odds.
+uint64_t mix64(uint64_t x) {
+    x ^= x >> 30;
+    x *= 0xBF58476D1CE4E5B9ull;
+    x ^= x >> 27;
+    x *= 0x94D049BB133111EBull;
+    x ^= x >> 31;
+    return x;
+}
+
+uint64_t elem_digest(uint32_t seed, uint64_t i, uint64_t v) {
+    return mix64(((uint64_t)seed << 56) ^ (i << 24) ^ (v * 0x9E3779B97F4A7C15ull));
+}
+
+template <class T>
+uint64_t array_digest(const T *a, uint64_t n, uint32_t seed) {
+    uint64_t acc = 0;
+    for (uint64_t i = 0; i < n; i++) acc += elem_digest(seed, i, a[i]);
+    return acc;
+}
+
+// A search result's digest: its first k hits as (pattern within the request,
+// offset) pairs of u32 (seed 7), then the per-pattern counts folded in, then
+// the total.
+uint64_t search_digest(const ol_hit *hits, uint64_t k, uint32_t pattern_base, const uint32_t *counts, uint32_t n,
+                       uint64_t total) {
+    uint64_t h = 0;
+    for (uint64_t j = 0; j < k; j++) {
+        h += elem_digest(7, 2 * j, hits[j].pattern - pattern_base);
+        h += elem_digest(7, 2 * j + 1, hits[j].offset);
+    }
+    for (uint32_t i = 0; i < n; i++) h = h * 0x100000001B3ull ^ counts[i];
+    return h ^ total;
 }
 
 struct Request {
@@ -46,6 +102,10 @@ struct Request {
     uint64_t doc_id = 0;
     std::vector<std::string> patterns;
     uint64_t submit_ns = 0;
+    bool has_pdest = false, has_sdest = false;
+    ol_parse_dest pdest{};
+    ol_search_dest sdest{};
+    uint64_t reserved = 0;  // bytes reserved in the store at admission
 };
 
 struct Entry {
@@ -56,6 +116,28 @@ struct Entry {
     uint64_t last_use = 0;
 };
 
+// Pinned host staging of one worker, grown on demand (never while copies into
+// it are in flight: every step reserves what it needs before enqueuing them).
+struct Staging {
+    uint8_t *ptr = nullptr;
+    uint64_t bytes = 0;
+    bool reserve(uint64_t need) {
+        if (need <= bytes) return true;
+        if (need > kStagingMaxBytes) return false;
+        const uint64_t want = std::min(kStagingMaxBytes, std::max<uint64_t>(need, bytes * 2));
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        if (cudaMallocHost((void **)&ptr, want) != cudaSuccess) {
+            cudaGetLastError();
+            ptr = nullptr;
+            return false;
+        }
+        bytes = want;
+        return true;
+    }
+};
+
 }  // namespace
 
 struct ol_server {
@@ -63,20 +145,23 @@ struct ol_server {
     uint32_t n_workers = 0;
     uint64_t budget = 0;
     uint64_t max_hits = 0;
+    uint32_t flags = 0;
     std::vector<ol_ctx *> ctxs;
+    std::vector<Staging> staging;
     std::vector<std::thread> threads;
     std::mutex qmu;
     std::condition_variable qcv;
     std::deque<Request *> queue;
     bool stopping = false;
+    bool paused = false;  // workers take no request while set (ol_server_pause)
     std::mutex rmu;
     std::condition_variable rcv;
     std::unordered_map<uint64_t, ol_request_result> results;
     std::atomic<uint64_t> next_id{1}, next_doc{1};
     std::mutex smu;
     std::unordered_map<uint64_t, Entry> store;
-    uint64_t used = 0, tick = 0;
-    std::atomic<uint64_t> evictions{0}, refusals{0};
+    uint64_t used = 0, reserved = 0, tick = 0;
+    std::atomic<uint64_t> evictions{0}, refusals{0}, steps{0}, served{0}, largest_step{0};
 };
 
 namespace {
@@ -86,17 +171,26 @@ uint64_t resident_bytes(const ol_doc *d) {
     return text + (uint64_t)d->line_cap * 6 + (uint64_t)d->line_count * 16;  // offsets, kinds, depth8; tree
 }
 
+// What a document of `len` bytes will hold in the store: its padded text, line
+// arrays for the estimated line count (with head room) and four tree arrays.
+uint64_t estimate_resident(const uint8_t *text, uint64_t len) {
+    if (len == 0) return 0;
+    const uint64_t lines = round_lines(estimate_lines(text, len));
+    return (uint64_t)parse_tiles(len) * kParseTile + kTextPad + lines * 22;
+}
+
 // Takes idle documents out of the store, least recently used first, until
-// `need` more bytes fit; the caller frees them after releasing smu (freeing
-// takes the owning context's lock, which a worker may hold while it waits for
-// smu). Called with smu held; returns false when the documents in use leave no
-// room.
+// `need` more bytes fit beside the documents in use and the reservations of
+// requests in flight; the caller frees them after releasing smu (freeing takes
+// the owning context's lock, which a worker may hold while it waits for smu).
+// Called with smu held; returns false, evicting nothing, when the documents in
+// use and the reservations leave no room.
 bool make_room(ol_server *s, uint64_t need, std::vector<Entry> &evicted) {
-    uint64_t busy = 0;  // documents in use cannot go: refuse before evicting anything
+    uint64_t busy = s->reserved;
     for (auto &kv : s->store)
         if (kv.second.refs) busy += kv.second.bytes;
     if (busy + need > s->budget) return false;
-    while (s->used + need > s->budget) {
+    while (s->used + s->reserved + need > s->budget) {
         uint64_t victim = 0, best = UINT64_MAX;
         for (auto &kv : s->store)
             if (kv.second.refs == 0 && kv.second.last_use < best) {
@@ -120,33 +214,40 @@ void free_entries(std::vector<Entry> &v) {
     v.clear();
 }
 
-void run_parse(ol_server *s, ol_ctx *ctx, unsigned long long *d_digest, Request *r, ol_request_result &res) {
-    ol_doc *d = nullptr;
-    ol_tree *t = nullptr;
-    ol_status st = ol_doc_upload(ctx, r->text, r->len, &d);
-    if (st == OL_OK) st = ol_tree_build(ctx, d, 0, &t);  // any depth
-    if (st == OL_OK) {
-        const uint32_t L = d->line_count;
-        cudaStream_t cs = ctx->stream;
-        unsigned long long h = 0;
-        cudaError_t e = cudaMemsetAsync(d_digest, 0, 8, cs);
-        if (e == cudaSuccess && L) e = launch_digest_u32(d->offsets, L, 1, d_digest, cs);
-        if (e == cudaSuccess && L) e = launch_digest_u8(d->kinds, L, 2, d_digest, cs);
-        const void *arr[4] = {t->parent_buf.ptr, t->end_buf.ptr, t->fc_buf.ptr, t->ns_buf.ptr};
-        for (uint32_t k = 0; k < 4 && e == cudaSuccess && L; k++)
-            e = launch_digest_u32((const uint32_t *)arr[k], L, 3 + k, d_digest, cs);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d_digest, 8, cudaMemcpyDeviceToHost, cs);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
-        if (e != cudaSuccess) st = ctx_cuda(ctx, e, "digest");
-        res.digest = h ^ ((uint64_t)L * 0x9E3779B97F4A7C15ull);
-        res.line_count = L;
-    }
+// A parsed document's six arrays in host memory.
+struct HostLines {
+    const uint32_t *offsets = nullptr;
+    const uint8_t *kinds = nullptr;
+    const uint32_t *links[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+// The result of a parse request from its arrays: the digest, and the arrays
+// into the caller's buffers when they have room for every line.
+void finish_parse(const Request *r, uint64_t L, const HostLines &h, ol_request_result &res) {
+    uint64_t dg = array_digest(h.offsets, L, 1) + array_digest(h.kinds, L, 2);
+    for (int k = 0; k < 4; k++) dg += array_digest(h.links[k], L, 3 + k);
+    res.digest = dg ^ (L * 0x9E3779B97F4A7C15ull);
+    res.line_count = L;
+    if (!r->has_pdest || r->pdest.cap < L || L == 0) return;
+    const ol_parse_dest &d = r->pdest;
+    if (d.offsets) memcpy(d.offsets, h.offsets, L * 4);
+    if (d.kinds) memcpy(d.kinds, h.kinds, L);
+    uint32_t *outs[4] = {d.parent, d.subtree_end, d.first_child, d.next_sibling};
+    for (int k = 0; k < 4; k++)
+        if (outs[k]) memcpy(outs[k], h.links[k], L * 4);
+}
+
+// Puts a parsed document into the store (its reservation becomes its real
+// size), or refuses it when the real size does not fit after all.
+void commit_doc(ol_server *s, Request *r, ol_doc *&d, ol_tree *&t, ol_request_result &res) {
     std::vector<Entry> evicted;
-    if (st == OL_OK) {
-        const uint64_t bytes = resident_bytes(d);
+    {
         std::lock_guard<std::mutex> g(s->smu);
+        s->reserved -= r->reserved;
+        r->reserved = 0;
+        const uint64_t bytes = resident_bytes(d);
         if (!make_room(s, bytes, evicted)) {
-            st = OL_ERR_ADMISSION;
+            res.status = OL_ERR_ADMISSION;
             s->refusals++;
         } else {
             Entry e;
@@ -162,101 +263,318 @@ void run_parse(ol_server *s, ol_ctx *ctx, unsigned long long *d_digest, Request 
         }
     }
     free_entries(evicted);
-    if (t) ol_tree_free(t);
-    if (d) ol_doc_free(d);
-    res.status = st;
 }
 
-void run_search(ol_server *s, ol_ctx *ctx, unsigned long long *d_digest, ol_hit *d_hits, Request *r,
-                ol_request_result &res) {
-    Entry e;
-    {
-        std::lock_guard<std::mutex> g(s->smu);
-        auto it = s->store.find(r->doc_id);
-        if (it == s->store.end()) {
-            res.status = OL_ERR_NOT_FOUND;
-            return;
-        }
-        it->second.refs++;
-        it->second.last_use = s->tick++;
-        e = it->second;
+void release_reservation(ol_server *s, Request *r) {
+    std::lock_guard<std::mutex> g(s->smu);
+    s->reserved -= r->reserved;
+    r->reserved = 0;
+}
+
+uint64_t staged_bytes(const ol_doc *d) { return ((uint64_t)d->line_count * 21 + 63) & ~63ull; }
+
+// Enqueues the download of one resident document's six arrays into staging at
+// `at` (bytes), which the caller has reserved.
+void stage_doc(ol_ctx *ctx, Staging &stg, uint64_t &at, const ol_doc *d, const ol_tree *t, HostLines &h) {
+    const uint64_t L = d->line_count;
+    cudaStream_t st = ctx->stream;
+    uint32_t *offs = (uint32_t *)(stg.ptr + at);
+    uint32_t *links = offs + L;
+    uint8_t *kinds = (uint8_t *)(links + 4 * L);
+    const void *src[4] = {t->parent_buf.ptr, t->end_buf.ptr, t->fc_buf.ptr, t->ns_buf.ptr};
+    if (L) {
+        GpuPass pass(ctx, "download");
+        cudaMemcpyAsync(offs, d->offsets, L * 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(kinds, d->kinds, L, cudaMemcpyDeviceToHost, st);
+        for (int k = 0; k < 4; k++) cudaMemcpyAsync(links + k * L, src[k], L * 4, cudaMemcpyDeviceToHost, st);
     }
+    h.offsets = offs;
+    h.kinds = kinds;
+    for (int k = 0; k < 4; k++) h.links[k] = links + k * L;
+    at += staged_bytes(d);
+}
+
+// The admitted parse requests of one step: one resident document each, equal
+// to ol_doc_upload + ol_tree_build of that document alone.
+void run_parses(ol_server *s, ol_ctx *ctx, Staging &stg, std::vector<Request *> &reqs,
+                std::vector<ol_request_result *> &res) {
+    const size_t n = reqs.size();
+    std::vector<ol_doc *> docs(n, nullptr);
+    std::vector<ol_tree *> trees(n, nullptr);
+    std::vector<ol_status> st(n, OL_OK);
+    if (n == 1 || (s->flags & OL_SERVER_NO_COALESCE)) {
+        for (size_t i = 0; i < n; i++) {
+            st[i] = ol_doc_upload(ctx, reqs[i]->text, reqs[i]->len, &docs[i]);
+            if (st[i] == OL_OK) st[i] = ol_tree_build(ctx, docs[i], 0, &trees[i]);  // any depth
+        }
+    } else {
+        std::vector<const uint8_t *> parts(n);
+        std::vector<uint64_t> lens(n);
+        for (size_t i = 0; i < n; i++) {
+            parts[i] = reqs[i]->text;
+            lens[i] = reqs[i]->len;
+        }
+        ol_batch *b = nullptr;
+        ol_status bs = batch_from_parts(ctx, parts.data(), lens.data(), (uint32_t)n, &b);
+        if (bs == OL_OK) bs = ol_batch_build_trees(ctx, b);
+        if (bs == OL_OK) bs = batch_split(ctx, b, docs, trees);
+        if (b) ol_batch_free(b);
+        if (bs != OL_OK) {
+            docs.assign(n, nullptr);
+            trees.assign(n, nullptr);
+            for (size_t i = 0; i < n; i++) st[i] = bs;
+        }
+    }
+    // every document's downloads into staging reserved once, then one wait
+    std::vector<HostLines> host(n);
+    uint64_t at = 0, need = 64;
+    for (size_t i = 0; i < n; i++)
+        if (st[i] == OL_OK) need += staged_bytes(docs[i]);
+    if (!stg.reserve(need))
+        for (size_t i = 0; i < n; i++)
+            if (st[i] == OL_OK) st[i] = OL_ERR_OOM;
+    {
+        std::lock_guard<std::recursive_mutex> g(ctx->mu);
+        cudaSetDevice(ctx->device);
+        for (size_t i = 0; i < n; i++)
+            if (st[i] == OL_OK) stage_doc(ctx, stg, at, docs[i], trees[i], host[i]);
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) {
+            ol_status cs = ctx_cuda(ctx, e, "server download");
+            for (size_t i = 0; i < n; i++)
+                if (st[i] == OL_OK) st[i] = cs;
+        }
+    }
+    prof_mark(ctx, "server: parse step");
+    for (size_t i = 0; i < n; i++) {
+        Request *r = reqs[i];
+        res[i]->status = st[i];
+        if (st[i] == OL_OK) {
+            finish_parse(r, docs[i]->line_count, host[i], *res[i]);
+            commit_doc(s, r, docs[i], trees[i], *res[i]);
+        } else {
+            release_reservation(s, r);
+        }
+        if (trees[i]) ol_tree_free(trees[i]);
+        if (docs[i]) ol_doc_free(docs[i]);
+        res[i]->end_ns = now_ns();
+    }
+}
+
+// A search request inside a merged pass: its patterns are [first, first + n)
+// of the merged set.
+struct SearchPart {
+    Request *r;
+    ol_request_result *res;
+    uint32_t first = 0, n = 0;
+};
+
+uint64_t hit_cap_of(const ol_server *s, const Request *r) { return r->has_sdest ? r->sdest.max_hits : s->max_hits; }
+
+// One dictionary pass over a resident document for the merged patterns of
+// `parts`, with room for `hit_cap` hits in staging. When every hit a request
+// keeps fits, each request gets its slice of the (pattern, offset)-ordered
+// hits; otherwise *overflow is set and no result is written.
+ol_status search_pass(ol_server *s, ol_ctx *ctx, Staging &stg, const Entry &e, std::vector<SearchPart> &parts,
+                      uint64_t hit_cap, bool &overflow) {
     std::vector<const uint8_t *> p;
     std::vector<uint32_t> lens;
-    for (auto &x : r->patterns) {
-        p.push_back((const uint8_t *)x.data());
-        lens.push_back((uint32_t)x.size());
-    }
-    ol_status st;
-    {
-        std::lock_guard<std::recursive_mutex> cg(ctx->mu);  // released before smu is taken again
-        ol_patset *set = nullptr;
-        st = ol_patset_compile(ctx, e.doc, p.data(), lens.data(), (uint32_t)p.size(), &set);
-        std::vector<uint32_t> counts(p.size());
-        uint64_t total = 0;
-        HitDest dest;
-        dest.dev = d_hits;
-        if (st == OL_OK) st = many_run(ctx, e.doc, set, s->max_hits, 0, counts.data(), &total, dest, nullptr, nullptr, 0);
-        if (st == OL_OK) {
-            const uint64_t k = std::min<uint64_t>(total, s->max_hits);
-            unsigned long long h = 0;
-            cudaStream_t cs = ctx->stream;
-            cudaError_t ce = cudaMemsetAsync(d_digest, 0, 8, cs);
-            if (ce == cudaSuccess && k) ce = launch_digest_u32((const uint32_t *)d_hits, 2 * k, 7, d_digest, cs);
-            if (ce == cudaSuccess) ce = cudaMemcpyAsync(&h, d_digest, 8, cudaMemcpyDeviceToHost, cs);
-            if (ce == cudaSuccess) ce = cudaStreamSynchronize(cs);
-            if (ce != cudaSuccess) st = ctx_cuda(ctx, ce, "digest");
-            for (size_t i = 0; i < counts.size(); i++) h = h * 0x100000001B3ull ^ counts[i];  // counts on the host
-            res.digest = h ^ total;
-            res.total_hits = total;
+    for (auto &x : parts) {
+        x.first = (uint32_t)p.size();
+        x.n = (uint32_t)x.r->patterns.size();
+        for (auto &q : x.r->patterns) {
+            p.push_back((const uint8_t *)q.data());
+            lens.push_back((uint32_t)q.size());
         }
-        if (set) ol_patset_free(set);
     }
+    std::lock_guard<std::recursive_mutex> cg(ctx->mu);
+    cudaSetDevice(ctx->device);
+    ol_patset *set = nullptr;
+    ol_status st = ol_patset_compile(ctx, e.doc, p.data(), lens.data(), (uint32_t)p.size(), &set);
+    std::vector<uint32_t> counts(p.size());
+    uint64_t total = 0;
+    if (st == OL_OK && !stg.reserve(hit_cap * sizeof(ol_hit) + 64)) st = OL_ERR_OOM;
+    if (st == OL_OK) {
+        HitDest dest;
+        dest.host = (ol_hit *)stg.ptr;
+        st = many_run(ctx, e.doc, set, hit_cap, 0, counts.data(), &total, dest, nullptr, nullptr, 0);
+    }
+    if (set) ol_patset_free(set);
+    overflow = false;
+    if (st != OL_OK) return st;
+    // every request needs the hits up to the end of the part of its slice it keeps
+    uint64_t need = 0, at = 0;
+    for (auto &x : parts) {
+        uint64_t tot = 0;
+        for (uint32_t i = 0; i < x.n; i++) tot += counts[x.first + i];
+        need = std::max(need, at + std::min(tot, hit_cap_of(s, x.r)));
+        at += tot;
+    }
+    if (need > hit_cap) {
+        overflow = true;
+        return OL_OK;
+    }
+    const ol_hit *hits = (const ol_hit *)stg.ptr;
+    uint64_t base = 0;  // the request's first hit
+    for (auto &x : parts) {
+        Request *r = x.r;
+        ol_request_result &res = *x.res;
+        uint64_t tot = 0;
+        for (uint32_t i = 0; i < x.n; i++) tot += counts[x.first + i];
+        const uint64_t k = std::min(tot, hit_cap_of(s, r));
+        const ol_hit *mine = hits + base;
+        res.digest = search_digest(mine, k, x.first, counts.data() + x.first, x.n, tot);
+        res.total_hits = tot;
+        if (r->has_sdest) {
+            if (r->sdest.counts) memcpy(r->sdest.counts, counts.data() + x.first, (size_t)x.n * 4);
+            if (r->sdest.hits)
+                for (uint64_t j = 0; j < k; j++) r->sdest.hits[j] = ol_hit{mine[j].pattern - x.first, mine[j].offset};
+        }
+        res.status = OL_OK;
+        base += tot;
+    }
+    return OL_OK;
+}
+
+bool patterns_ok(const Request *r) {
+    if (r->patterns.empty() || r->patterns.size() > OL_MAX_DICT_PATTERNS) return false;
+    for (auto &q : r->patterns)
+        if (q.size() < OL_MIN_SET_PATTERN_LEN || q.size() > OL_MAX_SET_PATTERN_LEN) return false;
+    return true;
+}
+
+// The search requests of one step on one resident document: one merged pass,
+// or, when the merged hits outgrow the room, one pass per request.
+void run_search_group(ol_server *s, ol_ctx *ctx, Staging &stg, uint64_t doc_id, std::vector<SearchPart> &parts) {
+    Entry e;
+    bool found = false;
     {
         std::lock_guard<std::mutex> g(s->smu);
-        auto it = s->store.find(r->doc_id);
+        auto it = s->store.find(doc_id);
+        if (it != s->store.end()) {
+            it->second.refs++;
+            it->second.last_use = s->tick++;
+            e = it->second;
+            found = true;
+        }
+    }
+    if (!found) {
+        for (auto &x : parts) x.res->status = OL_ERR_NOT_FOUND;
+    } else {
+        uint64_t cap = 0;
+        for (auto &x : parts) cap += hit_cap_of(s, x.r);
+        cap = std::min<uint64_t>(std::max<uint64_t>(cap, kStagingBytes / sizeof(ol_hit)),
+                                 kStagingMaxBytes / sizeof(ol_hit) - 8);
+        bool overflow = false;
+        ol_status st = parts.size() > 1 ? search_pass(s, ctx, stg, e, parts, cap, overflow) : OL_OK;
+        if (st == OL_OK && (overflow || parts.size() == 1)) {
+            for (auto &x : parts) {
+                std::vector<SearchPart> one{x};
+                bool of1 = false;
+                ol_status s1 = search_pass(s, ctx, stg, e, one, hit_cap_of(s, x.r), of1);
+                if (s1 == OL_OK && of1) s1 = OL_ERR_OOM;  // a request alone always fits its own cap
+                x.res->status = s1;
+            }
+        } else if (st != OL_OK) {
+            for (auto &x : parts) x.res->status = st;
+        }
+        std::lock_guard<std::mutex> g(s->smu);
+        auto it = s->store.find(doc_id);
         if (it != s->store.end()) it->second.refs--;
     }
-    res.doc_id = r->doc_id;
-    res.status = st;
+    prof_mark(ctx, "server: search step");
+    for (auto &x : parts) {
+        x.res->doc_id = doc_id;
+        x.res->end_ns = now_ns();
+    }
+}
+
+// One step: the requests taken from the queue together.
+void run_step(ol_server *s, uint32_t w, std::vector<Request *> &step) {
+    ol_ctx *ctx = s->ctxs[w];
+    Staging &stg = s->staging[w];
+    std::vector<ol_request_result> res(step.size());
+    const uint64_t start = now_ns();
+    for (size_t i = 0; i < step.size(); i++) {
+        res[i] = ol_request_result{};
+        res[i].id = step[i]->id;
+        res[i].kind = step[i]->kind;
+        res[i].submit_ns = step[i]->submit_ns;
+        res[i].start_ns = start;
+        res[i].worker = w;
+        res[i].status = OL_ERR_CUDA;
+    }
+    // Admission of the parse requests, before any work.
+    std::vector<Request *> parses;
+    std::vector<ol_request_result *> parse_res;
+    std::vector<Entry> evicted;
+    {
+        std::lock_guard<std::mutex> g(s->smu);
+        for (size_t i = 0; i < step.size(); i++) {
+            Request *r = step[i];
+            if (r->kind != 0) continue;
+            const uint64_t need = estimate_resident(r->text, r->len);
+            if (!make_room(s, need, evicted)) {
+                res[i].status = OL_ERR_ADMISSION;
+                res[i].end_ns = now_ns();
+                s->refusals++;
+                continue;
+            }
+            r->reserved = need;
+            s->reserved += need;
+            parses.push_back(r);
+            parse_res.push_back(&res[i]);
+        }
+    }
+    free_entries(evicted);
+    if (!parses.empty()) run_parses(s, ctx, stg, parses, parse_res);
+    // Search requests, merged per document.
+    std::map<uint64_t, std::vector<SearchPart>> groups;
+    for (size_t i = 0; i < step.size(); i++) {
+        Request *r = step[i];
+        if (r->kind != 1) continue;
+        if (!patterns_ok(r)) {
+            res[i].status = OL_ERR_BAD_PATTERN;
+            res[i].doc_id = r->doc_id;
+            res[i].end_ns = now_ns();
+            continue;
+        }
+        groups[r->doc_id].push_back(SearchPart{r, &res[i]});
+    }
+    for (auto &kv : groups) run_search_group(s, ctx, stg, kv.first, kv.second);
+    for (Request *r : step) delete r;
+    {
+        std::lock_guard<std::mutex> g(s->rmu);
+        for (auto &x : res) s->results[x.id] = x;
+    }
+    s->rcv.notify_all();
+    s->steps++;
+    s->served += step.size();
+    uint64_t big = s->largest_step.load();
+    while (step.size() > big && !s->largest_step.compare_exchange_weak(big, step.size())) {
+    }
 }
 
 void worker(ol_server *s, uint32_t w) {
-    ol_ctx *ctx = s->ctxs[w];
     cudaSetDevice(s->device);
-    unsigned long long *d_digest = nullptr;
-    ol_hit *d_hits = nullptr;
-    cudaMalloc(&d_digest, 8);
-    if (s->max_hits) cudaMalloc(&d_hits, s->max_hits * sizeof(ol_hit));
+    const uint32_t limit = (s->flags & OL_SERVER_NO_COALESCE) ? 1u : kStepMaxRequests;
     for (;;) {
-        Request *r = nullptr;
+        std::vector<Request *> step;
         {
             std::unique_lock<std::mutex> lk(s->qmu);
-            s->qcv.wait(lk, [&] { return s->stopping || !s->queue.empty(); });
+            s->qcv.wait(lk, [&] { return s->stopping || (!s->paused && !s->queue.empty()); });
             if (s->queue.empty()) break;
-            r = s->queue.front();
-            s->queue.pop_front();
+            uint64_t parse_bytes = 0;
+            while (!s->queue.empty() && step.size() < limit) {
+                Request *r = s->queue.front();
+                if (!step.empty() && r->kind == 0 && parse_bytes + r->len > kStepMaxParseBytes) break;
+                if (r->kind == 0) parse_bytes += r->len;
+                step.push_back(r);
+                s->queue.pop_front();
+            }
         }
-        ol_request_result res{};
-        res.id = r->id;
-        res.kind = r->kind;
-        res.submit_ns = r->submit_ns;
-        res.start_ns = now_ns();
-        res.worker = w;
-        if (r->kind == 0)
-            run_parse(s, ctx, d_digest, r, res);
-        else
-            run_search(s, ctx, d_digest, d_hits, r, res);
-        res.end_ns = now_ns();
-        delete r;
-        {
-            std::lock_guard<std::mutex> g(s->rmu);
-            s->results[res.id] = res;
-        }
-        s->rcv.notify_all();
+        run_step(s, w, step);
     }
-    cudaFree(d_digest);
-    if (d_hits) cudaFree(d_hits);
 }
 
 ol_status submit(ol_server *s, Request *r, uint64_t *id) {
@@ -277,20 +595,28 @@ ol_status submit(ol_server *s, Request *r, uint64_t *id) {
 
 }  // namespace
 
-extern "C" ol_status ol_server_create(int32_t device, uint32_t workers, uint64_t store_budget, uint64_t max_hits,
-                                      ol_server **out) {
-    if (!out || workers == 0 || workers > 64) return OL_ERR_INVALID_ARG;
+extern "C" ol_status ol_server_create_ex(int32_t device, uint32_t workers, uint64_t store_budget, uint64_t max_hits,
+                                         uint32_t flags, ol_server **out) {
+    if (!out || workers == 0 || workers > 64 || (flags & ~(uint32_t)OL_SERVER_NO_COALESCE)) return OL_ERR_INVALID_ARG;
     *out = nullptr;
     auto s = new ol_server();
     s->device = device;
     s->n_workers = workers;
     s->budget = store_budget;
     s->max_hits = max_hits;
+    s->flags = flags;
+    s->staging.resize(workers);
     for (uint32_t w = 0; w < workers; w++) {
         ol_ctx *c = nullptr;
         ol_status st = ol_ctx_create(device, &c);
+        if (st == OL_OK && !s->staging[w].reserve(kStagingBytes)) {
+            ol_ctx_destroy(c);
+            st = OL_ERR_OOM;  // the pinned staging could not be allocated: refuse to start
+        }
         if (st != OL_OK) {
             for (ol_ctx *x : s->ctxs) ol_ctx_destroy(x);
+            for (auto &g : s->staging)
+                if (g.ptr) cudaFreeHost(g.ptr);
             delete s;
             return st;
         }
@@ -314,6 +640,11 @@ extern "C" ol_status ol_server_create(int32_t device, uint32_t workers, uint64_t
     return OL_OK;
 }
 
+extern "C" ol_status ol_server_create(int32_t device, uint32_t workers, uint64_t store_budget, uint64_t max_hits,
+                                      ol_server **out) {
+    return ol_server_create_ex(device, workers, store_budget, max_hits, 0, out);
+}
+
 extern "C" void ol_server_destroy(ol_server *s) {
     if (!s) return;
     {
@@ -328,26 +659,48 @@ extern "C" void ol_server_destroy(ol_server *s) {
     }
     s->store.clear();
     for (ol_ctx *c : s->ctxs) ol_ctx_destroy(c);
+    for (auto &g : s->staging)
+        if (g.ptr) cudaFreeHost(g.ptr);
     delete s;
 }
 
-extern "C" ol_status ol_server_submit_parse(ol_server *s, const uint8_t *text, uint64_t len, uint64_t *request_id) {
+extern "C" ol_status ol_server_submit_parse_to(ol_server *s, const uint8_t *text, uint64_t len,
+                                               const ol_parse_dest *dest, uint64_t *request_id) {
     if (!s || !request_id || (len && !text)) return OL_ERR_INVALID_ARG;
+    if (len > OL_MAX_GPU_INPUT_LEN) return OL_ERR_INPUT_TOO_LARGE;
     auto r = new Request();
     r->kind = 0;
     r->text = text;
     r->len = len;
+    if (dest) {
+        r->has_pdest = true;
+        r->pdest = *dest;
+    }
     return submit(s, r, request_id);
 }
 
-extern "C" ol_status ol_server_submit_search(ol_server *s, uint64_t doc_id, const uint8_t *const *patterns,
-                                             const uint32_t *lens, uint32_t n, uint64_t *request_id) {
+extern "C" ol_status ol_server_submit_parse(ol_server *s, const uint8_t *text, uint64_t len, uint64_t *request_id) {
+    return ol_server_submit_parse_to(s, text, len, nullptr, request_id);
+}
+
+extern "C" ol_status ol_server_submit_search_to(ol_server *s, uint64_t doc_id, const uint8_t *const *patterns,
+                                                const uint32_t *lens, uint32_t n, const ol_search_dest *dest,
+                                                uint64_t *request_id) {
     if (!s || !request_id || !n || !patterns || !lens) return OL_ERR_INVALID_ARG;
     auto r = new Request();
     r->kind = 1;
     r->doc_id = doc_id;
     for (uint32_t i = 0; i < n; i++) r->patterns.emplace_back((const char *)patterns[i], lens[i]);
+    if (dest) {
+        r->has_sdest = true;
+        r->sdest = *dest;
+    }
     return submit(s, r, request_id);
+}
+
+extern "C" ol_status ol_server_submit_search(ol_server *s, uint64_t doc_id, const uint8_t *const *patterns,
+                                             const uint32_t *lens, uint32_t n, uint64_t *request_id) {
+    return ol_server_submit_search_to(s, doc_id, patterns, lens, n, nullptr, request_id);
 }
 
 extern "C" ol_status ol_server_wait(ol_server *s, uint64_t request_id, ol_request_result *out) {
@@ -367,5 +720,23 @@ extern "C" ol_status ol_server_stats(ol_server *s, uint64_t *resident_docs, uint
     if (resident_bytes_out) *resident_bytes_out = s->used;
     if (evictions) *evictions = s->evictions;
     if (refusals) *refusals = s->refusals;
+    return OL_OK;
+}
+
+extern "C" ol_status ol_server_pause(ol_server *s, uint32_t paused) {
+    if (!s) return OL_ERR_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> g(s->qmu);
+        s->paused = paused != 0;
+    }
+    s->qcv.notify_all();
+    return OL_OK;
+}
+
+extern "C" ol_status ol_server_steps(ol_server *s, uint64_t *steps, uint64_t *requests, uint64_t *largest_step) {
+    if (!s) return OL_ERR_INVALID_ARG;
+    if (steps) *steps = s->steps;
+    if (requests) *requests = s->served;
+    if (largest_step) *largest_step = s->largest_step;
     return OL_OK;
 }

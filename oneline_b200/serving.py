@@ -1,11 +1,15 @@
 """GpuServer: the serving loop of the CUDA library (ol_server_* in
 include/oneline_cuda.h), for parse and search requests of mixed sizes.
 
-Worker threads in the library each own a context and a stream; requests queue
-as they arrive and start as soon as a worker frees up, so their kernels overlap
-on the device. Parsed documents stay resident in an HBM-budgeted store and are
-searched without uploading their text again. No reference counterpart: the
-reference offers one blocking call per document (crates/oneline-gpu/src/parser.rs).
+Worker threads in the library each own a context and a stream. A worker that
+frees up takes every queued request and serves them as one step (continuous
+batching): parse requests are admitted against the HBM budget before any
+upload, then parsed and linked as one batch; searches of the same document
+share one dictionary pass. Steps of different workers overlap on the device.
+Parsed documents stay resident in the budgeted store and are searched without
+uploading their text again. Results are downloaded into the caller's arrays
+before a request completes. No reference counterpart: the reference offers one
+blocking call per document (crates/oneline-gpu/src/parser.rs).
 """
 from __future__ import annotations
 
@@ -32,35 +36,87 @@ class RequestResult(ctypes.Structure):
         return int(self.end_ns - self.submit_ns)
 
 
+class ParseDest(ctypes.Structure):
+    """ol_parse_dest."""
+
+    _fields_ = [("cap", ctypes.c_uint64), ("offsets", ctypes.c_void_p), ("kinds", ctypes.c_void_p),
+                ("parent", ctypes.c_void_p), ("subtree_end", ctypes.c_void_p), ("first_child", ctypes.c_void_p),
+                ("next_sibling", ctypes.c_void_p)]
+
+
+class SearchDest(ctypes.Structure):
+    """ol_search_dest."""
+
+    _fields_ = [("max_hits", ctypes.c_uint64), ("counts", ctypes.c_void_p), ("hits", ctypes.c_void_p)]
+
+
+NO_COALESCE = 1  # OL_SERVER_NO_COALESCE
+HIT_DTYPE = np.dtype([("pattern", "<u4"), ("offset", "<u4")])
+LINK_NAMES = ("parent", "subtree_end", "first_child", "next_sibling")
+
+
 class GpuServer:
-    def __init__(self, device: int = 0, workers: int = 8, store_budget: int = 4 << 30, max_hits: int = 1 << 22):
+    """The serving loop. ``coalesce=False`` serves one request per step (the
+    plain per-request form)."""
+
+    def __init__(self, device: int = 0, workers: int = 8, store_budget: int = 4 << 30, max_hits: int = 1 << 22,
+                 coalesce: bool = True):
         h = ctypes.c_void_p()
-        st = _lib.load().ol_server_create(device, workers, store_budget, max_hits, ctypes.byref(h))
+        st = _lib.load().ol_server_create_ex(device, workers, store_budget, max_hits, 0 if coalesce else NO_COALESCE,
+                                             ctypes.byref(h))
         if st != 0:
             raise OnelineError(st, "could not start the server")
         self._h = h.value
+        self.max_hits = max_hits
         self._keep = {}  # request id -> buffers that must outlive the request
+        self._out = {}   # request id -> result arrays
 
-    def submit_parse(self, text) -> int:
+    def submit_parse(self, text, *, results: bool = False, cap: int | None = None) -> int:
+        """Queues a parse. With ``results``, the document's offsets, kinds and four
+        tree arrays come back with the result (``cap`` lines of room; default: one
+        line per byte, always enough)."""
         buf = np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray)) else np.ascontiguousarray(text, np.uint8)
         rid = ctypes.c_uint64()
-        st = _lib.load().ol_server_submit_parse(self._h, buf.ctypes.data, buf.size, ctypes.byref(rid))
+        dest, out = None, None
+        if results:
+            n = int(cap if cap is not None else buf.size + 1)
+            out = {"offsets": np.zeros(max(n, 1), np.uint32), "kinds": np.zeros(max(n, 1), np.uint8)}
+            for k in LINK_NAMES:
+                out[k] = np.zeros(max(n, 1), np.uint32)
+            dest = ParseDest(n, *[out[k].ctypes.data for k in ("offsets", "kinds") + LINK_NAMES])
+        st = _lib.load().ol_server_submit_parse_to(self._h, buf.ctypes.data, buf.size,
+                                                   ctypes.byref(dest) if dest is not None else None,
+                                                   ctypes.byref(rid))
         if st != 0:
             raise OnelineError(st, "submit_parse")
-        self._keep[rid.value] = buf
+        self._keep[rid.value] = (buf, dest)
+        if out is not None:
+            self._out[rid.value] = out
         return rid.value
 
-    def submit_search(self, doc_id: int, patterns) -> int:
+    def submit_search(self, doc_id: int, patterns, *, results: bool = False, max_hits: int | None = None) -> int:
+        """Queues a search of a resident document. With ``results``, the counts
+        and the first ``max_hits`` hits (pattern = index in ``patterns``) come back."""
         pats = [bytes(p) for p in patterns]
         bufs = [np.frombuffer(p, np.uint8) for p in pats]
         P = (ctypes.c_void_p * len(pats))(*[b.ctypes.data for b in bufs])
         lens = np.array([len(p) for p in pats], np.uint32)
         rid = ctypes.c_uint64()
-        st = _lib.load().ol_server_submit_search(self._h, int(doc_id), P, lens.ctypes.data, len(pats),
-                                                 ctypes.byref(rid))
+        dest, out = None, None
+        if results:
+            mh = int(max_hits if max_hits is not None else self.max_hits)
+            out = {"counts": np.zeros(max(len(pats), 1), np.uint32), "hits": np.zeros(max(mh, 1), HIT_DTYPE)}
+            dest = SearchDest(mh, out["counts"].ctypes.data, out["hits"].ctypes.data)
+        st = _lib.load().ol_server_submit_search_to(self._h, int(doc_id), P, lens.ctypes.data, len(pats),
+                                                    ctypes.byref(dest) if dest is not None else None,
+                                                    ctypes.byref(rid))
         if st != 0:
             raise OnelineError(st, "submit_search")
-        return rid.value  # the patterns are copied at submission
+        self._keep[rid.value] = dest  # the patterns are copied at submission
+        if out is not None:
+            out["n_patterns"] = len(pats)
+            self._out[rid.value] = out
+        return rid.value
 
     def wait(self, request_id: int) -> RequestResult:
         r = RequestResult()
@@ -70,10 +126,33 @@ class GpuServer:
         self._keep.pop(request_id, None)
         return r
 
+    def results(self, request_id: int, result: RequestResult) -> dict | None:
+        """The arrays of a finished request submitted with ``results=True``, cut to
+        their lengths (None when it failed or its arrays had no room)."""
+        out = self._out.pop(request_id, None)
+        if out is None or result.status != 0:
+            return None
+        if result.kind == KIND_PARSE:
+            L = int(result.line_count)
+            if L > out["offsets"].size:
+                return None
+            return {k: v[:L] for k, v in out.items()}
+        k = min(int(result.total_hits), out["hits"].size)
+        return {"counts": out["counts"][: out["n_patterns"]], "hits": out["hits"][:k]}
+
     def stats(self) -> dict:
         v = [ctypes.c_uint64() for _ in range(4)]
         _lib.load().ol_server_stats(self._h, *[ctypes.byref(x) for x in v])
         return dict(zip(("resident_docs", "resident_bytes", "evictions", "refusals"), (int(x.value) for x in v)))
+
+    def pause(self, paused: bool = True) -> None:
+        """Workers take no new request while paused (requests still queue)."""
+        _lib.load().ol_server_pause(self._h, 1 if paused else 0)
+
+    def steps(self) -> dict:
+        v = [ctypes.c_uint64() for _ in range(3)]
+        _lib.load().ol_server_steps(self._h, *[ctypes.byref(x) for x in v])
+        return dict(zip(("steps", "requests", "largest_step"), (int(x.value) for x in v)))
 
     def close(self) -> None:
         if self._h:

@@ -78,3 +78,80 @@ def test_store_budget_evicts_and_refuses():
         assert kept.status == 0 and kept.total_hits > 0
         r = s.wait(s.submit_parse(big))
         assert r.status == OL_ERR_ADMISSION and s.stats()["refusals"] == 1
+
+
+def test_queued_requests_share_launches_and_results_reach_the_caller():
+    """Continuous batching: requests queued together are served as one step,
+    with fewer kernel launches than the same requests served one at a time,
+    and every result (arrays in the caller's buffers, and digests) is the same
+    both ways and equal to the oracle's."""
+    from oneline_b200 import _lib
+
+    L = _lib.load()
+    texts, searches = workload()
+    want_parse, want_search = oracle_digests(texts, searches)
+    runs = {}
+    for coalesce in (False, True):
+        with GpuServer(workers=1, store_budget=1 << 30, coalesce=coalesce) as s:
+            s.pause()
+            l0 = L.ol_launch_count()
+            pids = [s.submit_parse(t, results=True) for t in texts]
+            s.pause(False)
+            parsed = [s.wait(r) for r in pids]
+            arrays = [s.results(r, res) for r, res in zip(pids, parsed)]
+            l1 = L.ol_launch_count()
+            s.pause()
+            sids = [s.submit_search(parsed[i].doc_id, pats, results=True) for i, pats in searches]
+            # a second request on each document, so searches of one document share a pass
+            sids2 = [s.submit_search(parsed[i].doc_id, pats) for i, pats in searches]
+            s.pause(False)
+            found = [s.wait(r) for r in sids]
+            found2 = [s.wait(r) for r in sids2]
+            hits = [s.results(r, res) for r, res in zip(sids, found)]
+            l2 = L.ol_launch_count()
+            runs[coalesce] = dict(parse_launches=l1 - l0, search_launches=l2 - l1, steps=s.steps(),
+                                  parsed=parsed, arrays=arrays, found=found, found2=found2, hits=hits)
+    plain, batched = runs[False], runs[True]
+    n_req = len(texts) + 2 * len(searches)
+    assert plain["steps"]["largest_step"] == 1 and plain["steps"]["steps"] == n_req
+    assert batched["steps"]["steps"] < n_req and batched["steps"]["largest_step"] > 1
+    assert batched["parse_launches"] < len(texts) * 2 < plain["parse_launches"]
+    assert batched["search_launches"] < plain["search_launches"] / 4
+    for run in (plain, batched):
+        assert all(r.status == 0 for r in run["parsed"] + run["found"] + run["found2"])
+        assert [r.digest for r in run["parsed"]] == want_parse
+        assert [r.digest for r in run["found"]] == want_search == [r.digest for r in run["found2"]]
+    for t, a in zip(texts, batched["arrays"]):
+        offs, nodes = oracle.parse(t)
+        tr = oracle.full_tree(nodes)
+        assert np.array_equal(a["offsets"], offs) and np.array_equal(a["kinds"], nodes["kind"].astype(np.uint8))
+        for k in ("parent", "subtree_end", "first_child", "next_sibling"):
+            assert np.array_equal(a[k], tr[k]), k
+    for (i, pats), h in zip(searches, batched["hits"]):
+        counts, hp, ho = oracle.find_many(texts[i], pats)
+        assert np.array_equal(h["counts"], counts.astype(np.uint32))
+        assert np.array_equal(h["hits"]["pattern"], hp) and np.array_equal(h["hits"]["offset"], ho)
+
+
+def test_admission_is_decided_before_any_work_and_counts_requests_in_flight():
+    from oneline_b200 import _lib
+
+    L = _lib.load()
+    a = datagen.corpus(4 << 20, 11).tobytes()
+    b = datagen.corpus(4 << 20, 12).tobytes()
+    huge = datagen.corpus(12 << 20, 13).tobytes()
+    with GpuServer(workers=1, store_budget=8 << 20) as s:
+        l0 = L.ol_launch_count()
+        r = s.wait(s.submit_parse(huge))
+        assert r.status == OL_ERR_ADMISSION and L.ol_launch_count() == l0  # refused without a kernel
+        # a and b fit one at a time, not together: in one step, b is refused
+        # because a's reservation counts although a is not yet in the store
+        s.pause()
+        ra, rb = s.submit_parse(a), s.submit_parse(b)
+        s.pause(False)
+        res_a, res_b = s.wait(ra), s.wait(rb)
+        assert res_a.status == 0 and res_b.status == OL_ERR_ADMISSION
+        assert s.stats()["refusals"] == 2 and s.stats()["resident_bytes"] <= 8 << 20
+        # alone, b fits (a, idle, is evicted)
+        res_b2 = s.wait(s.submit_parse(b))
+        assert res_b2.status == 0 and s.stats()["evictions"] == 1
