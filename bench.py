@@ -97,7 +97,9 @@ def parse_args():
                          "serve: open-loop Poisson parse/search requests, concurrent workers vs one")
     ap.add_argument("--pattern-source-bytes", type=int, default=0,
                     help="sample the 8 patterns from the document of this size (the text is its prefix)")
-    ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the serve workload's arrival stream")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="length of the serve workload's arrival stream")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch sub-record of the default workload")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serve sub-record of the default workload")
     ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean arrivals per second")
     return ap.parse_args()
@@ -626,12 +628,18 @@ def run_ours(args, world, rank, local):
             parity["ranks_mismatched"] = int(bad)
         del port
 
-    dict_rec = None
-    if not args.no_dictionary:
-        if not args.no_graph:
-            pipe.free()
-        del outs
+    # Sub-records of the other workloads, at N = 1 only (a scaling run times the
+    # headline alone).
+    dict_rec = batch_rec = serve_rec = None
+    if not args.no_graph:
+        pipe.free()
+    del outs
+    if world == 1 and not args.no_dictionary:
         dict_rec = dictionary_record(args, world, rank, local, p)
+    if world == 1 and not args.no_batch:
+        batch_rec = batch_record(args, world, rank, local, p)
+    if world == 1 and not args.no_serve:
+        serve_rec = serve_record(args, local)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -641,7 +649,7 @@ def run_ours(args, world, rank, local):
                 "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "e2e": e2e,
                 "gpu_launches": int(launches), "clocks": clocks.summary(),
                 "step_form": "CUDA graph (ol_pipeline_launch)" if not args.no_graph else "enqueued calls",
-                "dictionary": dict_rec, "device": p.adapter_name()}
+                "dictionary": dict_rec, "batch": batch_rec, "serve": serve_rec, "device": p.adapter_name()}
         print(json.dumps(line), flush=True)
 
 
@@ -867,7 +875,7 @@ def run_dictionary(args, world, rank, local):
 
 # ----------------------------------------------------------------- batch
 
-def run_batch(args, world, rank, local):
+def batch_record(args, world, rank, local, p=None) -> dict:
     """10,000 documents (seeds 3..10002, log-normal sizes, median 16 KiB, sigma 1.5,
     256 B..64 MiB): full parse, tree links and a 1,000-pattern dictionary search of
     every document, batched (one upload, one parse, one tree build, one search) vs
@@ -888,7 +896,7 @@ def run_batch(args, world, rank, local):
     pats = datagen.patterns_dictionary(dict_text, 2, n=10_000)[:1000]
     del dict_text
     torch.cuda.set_device(local)
-    p = GpuParser(local)
+    p = p or GpuParser(local)
     data = torch.empty(total_bytes, dtype=torch.uint8, pin_memory=True)
     data.numpy()[:] = data_np
     ps = p.compile_patterns(None, pats)
@@ -950,6 +958,7 @@ def run_batch(args, world, rank, local):
     assert got_plain == total, (got_plain, total)
     bytes_all = allreduce_sum(float(total_bytes), world)
     value = bytes_all / dt / 1e9
+    line = {}
     if rank == 0:
         plain_v = bytes_all / dt_plain / 1e9
         line = {"metric": "batched parse+dictionary GB/s vs one call per document", "value": round(value, 3),
@@ -968,7 +977,14 @@ def run_batch(args, world, rank, local):
                         "d2h_bytes_per_step": 4 * len(pats) + 8,
                         "timing": "host wall clock around the blocking batch calls (the value itself)",
                         "path": "ol_batch_upload (pinned) + ol_batch_build_trees + ol_batch_search_many (hits in HBM)"},
-                "gpu_launches": int(launches), "clocks": clocks.summary(), "device": p.adapter_name()}
+                "gpu_launches": int(launches), "launches_per_step": round(launches / max(args.steps, 1), 1),
+                "clocks": clocks.summary(), "device": p.adapter_name()}
+    return line
+
+
+def run_batch(args, world, rank, local):
+    line = batch_record(args, world, rank, local)
+    if rank == 0:
         print(json.dumps(line), flush=True)
 
 
@@ -1000,14 +1016,19 @@ def serve_stream(seconds: float, seed: int = 4, rate: float = 2000.0):
     return reqs, base
 
 
-def serve_run(reqs, workers: int, warm_docs):
+SERVE_MAX_HITS = 1 << 18  # hits a search request gets back
+
+
+def serve_run(reqs, workers: int, warm_docs, coalesce: bool):
     """Plays the stream open-loop against a server; returns per-request latencies
-    and the bytes processed."""
+    and the bytes processed. Every request gets its results back in host arrays
+    (a parse: offsets, kinds and the four tree arrays; a search: counts and up
+    to SERVE_MAX_HITS hits), so the latency covers the download."""
     import threading
 
     from oneline_b200.serving import GpuServer
 
-    with GpuServer(workers=workers, store_budget=4 << 30, max_hits=1 << 22) as srv:
+    with GpuServer(workers=workers, store_budget=4 << 30, max_hits=SERVE_MAX_HITS, coalesce=coalesce) as srv:
         # warm-up outside the timed stream: resident documents to search, and
         # every kernel launched once (the first launch of a kernel loads it)
         ready = [srv.wait(r).doc_id for r in [srv.submit_parse(d) for d in warm_docs]]
@@ -1033,6 +1054,7 @@ def serve_run(reqs, workers: int, warm_docs):
                     continue
                 rid, kind, nbytes = item
                 r = srv.wait(rid)
+                srv.results(rid, r)  # the arrays are in host memory; release them
                 if kind == "parse" and r.status == 0:
                     with lock:
                         ready.append(r.doc_id)
@@ -1049,33 +1071,37 @@ def serve_run(reqs, workers: int, warm_docs):
             if delay > 0:
                 time.sleep(delay)
             if req[0] == "parse":
-                rid = srv.submit_parse(req[2])
+                rid = srv.submit_parse(req[2], results=True, cap=int(req[2].size) // 8 + 4096)
                 with lock:
                     pending.append((rid, "parse", int(req[2].size)))
             else:
                 with lock:
                     doc = ready[req[3] % len(ready)]
-                rid = srv.submit_search(doc, req[2])
+                rid = srv.submit_search(doc, req[2], results=True)
                 with lock:
                     pending.append((rid, "search", 0))
         done.set()
         col.join()
         wall = time.perf_counter() - t0
-        stats = srv.stats()
+        stats = {**srv.stats(), **srv.steps()}
     return results, wall, stats
 
 
-def run_serve(args, world, rank, local):
-    if rank != 0:
-        return
-    from oneline_b200 import GpuParser, datagen
+def serve_record(args, local) -> dict:
+    """The serving workload: the same open-loop stream against the served form
+    (`serve_workers` workers, continuous batching) and the plain form (one
+    worker, one request per step: every request its own launches)."""
+    from oneline_b200 import GpuParser, _lib
 
+    L = _lib.load()
     reqs, base = serve_stream(args.serve_seconds, rate=args.serve_rate)
     warm = [base[i << 20: (i << 20) + (64 << 10)] for i in range(64)]
     out = {}
-    for name, workers in (("served", args.serve_workers), ("plain", 1)):
+    for name, workers, coalesce in (("served", args.serve_workers, True), ("plain", 1, False)):
+        l0 = L.ol_launch_count()
         with ClockSampler(local) as clocks:
-            res, wall, stats = serve_run(reqs, workers, warm)
+            res, wall, stats = serve_run(reqs, workers, warm, coalesce)
+        launches = L.ol_launch_count() - l0
         ok = [r for r in res if r[1] == 0]
         lat = np.array([r[2] for r in ok], np.float64) / 1e6
         wait = np.array([r[4] - r[6] for r in ok], np.float64) / 1e6  # queued before a worker took it
@@ -1083,7 +1109,8 @@ def run_serve(args, world, rank, local):
         by_kind = {k: np.array([r[2] for r in ok if r[0] == k], np.float64) / 1e6 for k in ("parse", "search")}
         span = (max(r[5] for r in ok) - min(r[6] for r in ok)) / 1e9
         nbytes = sum(r[3] for r in ok)
-        out[name] = {"workers": workers, "requests": len(res), "ok": len(ok),
+        out[name] = {"workers": workers, "coalesce": coalesce, "requests": len(res), "ok": len(ok),
+                     "gpu_launches": int(launches), "launches_per_request": round(launches / max(len(res), 1), 2),
                      "refused": sum(1 for r in res if r[1] == 6), "not_found": sum(1 for r in res if r[1] == 9),
                      "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
                      "queue_p99_ms": round(float(np.percentile(wait, 99)), 3),
@@ -1093,7 +1120,7 @@ def run_serve(args, world, rank, local):
                      "req_per_s": round(len(ok) / wall, 1), "gb_per_s": round(nbytes / span / 1e9, 3),
                      "wall_s": round(wall, 2), "store": stats, "clocks": clocks.summary()}
     sv, pl = out["served"], out["plain"]
-    line = {"metric": "served req/s at p99 vs per-request launches", "value": sv["req_per_s"], "unit": "req/s",
+    return {"metric": "served req/s at p99 vs per-request launches", "value": sv["req_per_s"], "unit": "req/s",
             "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": round(sv["wall_s"] * 1e3, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": {"workload": f"open-loop Poisson stream, {args.serve_rate:g} req/s for {args.serve_seconds} s: 30% parse "
@@ -1103,8 +1130,14 @@ def run_serve(args, world, rank, local):
             "served": sv, "plain": pl,
             "p99_speedup_vs_plain": round(pl["p99_ms"] / max(sv["p99_ms"], 1e-9), 2),
             "gbps_vs_plain": round(sv["gb_per_s"] / max(pl["gb_per_s"], 1e-9), 2),
+            "results": "every request's arrays downloaded to host memory before it completes",
             "device": GpuParser(local).adapter_name()}
-    print(json.dumps(line), flush=True)
+
+
+def run_serve(args, world, rank, local):
+    if rank != 0:
+        return
+    print(json.dumps(serve_record(args, local)), flush=True)
 
 
 def main():

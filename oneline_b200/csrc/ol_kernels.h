@@ -41,10 +41,19 @@ struct ParseArgs {
     uint32_t *redo_n;
     uint32_t *redo_list;
     uint32_t slot_cap;
+    uint32_t first_tile;  // staged pass 1: block b takes tile first_tile + b (launches over tile ranges)
 };
 constexpr uint32_t kParseSlotCap = 1024;  // staged lines per tile
 
 cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st);
+// The staged form in three parts, for a parse that starts while the text is
+// still arriving: begin (reset the redo list), the stage pass over tiles
+// [t0, t1) (any ranges that together cover every tile once, each launched once
+// its tiles and their 256-byte halo are in device memory), then end (the scan,
+// the copy pass, the redo and fix-up passes).
+cudaError_t launch_parse_begin(const ParseArgs &a, cudaStream_t st);
+cudaError_t launch_parse_tiles(const ParseArgs &a, uint32_t t0, uint32_t t1, cudaStream_t st);
+cudaError_t launch_parse_end(const ParseArgs &a, cudaStream_t st);
 
 // Exclusive scan of each of `cols` columns of a column-major u32 matrix:
 // column c is `rows` entries at in + c * ld (in, out 16-byte aligned, ld a

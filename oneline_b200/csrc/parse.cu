@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a)
 // Staged form, pass 1: every tile counts its newlines and stages its lines.
 __global__ void __launch_bounds__(PT_THREADS, 6) parse_stage_kernel(ParseArgs a) {
     __shared__ ParseSmem sm;
-    parse_tile<true>(a, sm, blockIdx.x);
+    parse_tile<true>(a, sm, a.first_tile + blockIdx.x);
 }
 
 // Staged form, pass 3: the tiles listed by pass 1 (more lines than a slot
@@ -445,13 +445,9 @@ cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st) {
     cudaError_t e;
     if (a.slot) {
         // staged: the text is read once; tiles with too many lines are redone
-        if (a.slot_cap > PT_LIST) return cudaErrorInvalidValue;  // a slot is listed in one round
-        if ((e = cudaMemsetAsync(a.redo_n, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
-        parse_stage_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a); OL_LAUNCHED();
-        e = launch_scan_columns(a.tile_count, a.tile_base, nullptr, a.n_tiles, 1, scan_ld(a.n_tiles), st);
-        if (e != cudaSuccess) return e;
-        parse_copy_kernel<<<(a.n_tiles + PC_TILES - 1) / PC_TILES, 256, 0, st>>>(a); OL_LAUNCHED();
-        parse_redo_kernel<<<std::min(a.n_tiles, 512u), PT_THREADS, 0, st>>>(a); OL_LAUNCHED();
+        if ((e = launch_parse_begin(a, st)) != cudaSuccess) return e;
+        if ((e = launch_parse_tiles(a, 0, a.n_tiles, st)) != cudaSuccess) return e;
+        return launch_parse_end(a, st);
     } else {
         newline_count_kernel<<<a.n_tiles, PT_THREADS, 0, st>>>(a.text, a.text_len, a.tile_count); OL_LAUNCHED();
         e = launch_scan_columns(a.tile_count, a.tile_base, nullptr, a.n_tiles, 1, scan_ld(a.n_tiles), st);
@@ -461,6 +457,33 @@ cudaError_t launch_parse(const ParseArgs &a, cudaStream_t st) {
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     uint32_t blocks = a.fixup_cap < 64 ? 8 : 64;
+    parse_fixup_kernel<<<blocks, 256, 0, st>>>(a); OL_LAUNCHED();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_parse_begin(const ParseArgs &a, cudaStream_t st) {
+    if (!a.slot || a.slot_cap > PT_LIST) return cudaErrorInvalidValue;  // a slot is listed in one round
+    return cudaMemsetAsync(a.redo_n, 0, sizeof(uint32_t), st);
+}
+
+cudaError_t launch_parse_tiles(const ParseArgs &a, uint32_t t0, uint32_t t1, cudaStream_t st) {
+    t1 = std::min(t1, a.n_tiles);
+    if (t0 >= t1) return cudaSuccess;
+    ParseArgs r = a;
+    r.first_tile = t0;
+    parse_stage_kernel<<<t1 - t0, PT_THREADS, 0, st>>>(r); OL_LAUNCHED();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_parse_end(const ParseArgs &a, cudaStream_t st) {
+    if (a.n_tiles == 0) return cudaSuccess;
+    cudaError_t e = launch_scan_columns(a.tile_count, a.tile_base, nullptr, a.n_tiles, 1, scan_ld(a.n_tiles), st);
+    if (e != cudaSuccess) return e;
+    parse_copy_kernel<<<(a.n_tiles + PC_TILES - 1) / PC_TILES, 256, 0, st>>>(a); OL_LAUNCHED();
+    parse_redo_kernel<<<std::min(a.n_tiles, 512u), PT_THREADS, 0, st>>>(a); OL_LAUNCHED();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const uint32_t blocks = a.fixup_cap < 64 ? 8 : 64;
     parse_fixup_kernel<<<blocks, 256, 0, st>>>(a); OL_LAUNCHED();
     return cudaGetLastError();
 }

@@ -50,12 +50,12 @@ void release(Prof *p) {
 }
 }  // namespace
 
-GpuPass::GpuPass(ol_ctx *c, const char *label) : ctx(c) {
+GpuPass::GpuPass(ol_ctx *c, const char *label, cudaStream_t on) : ctx(c), stream(on ? on : (c ? c->stream : nullptr)) {
     Prof *p = c ? c->prof : nullptr;
-    if (!p || p->passes.size() >= OL_PROFILE_MAX_STEPS || capturing(c->stream)) return;
+    if (!p || p->passes.size() >= OL_PROFILE_MAX_STEPS || capturing(stream)) return;
     ProfPass x{label, nullptr, nullptr};
     if (cudaEventCreate(&x.start) != cudaSuccess || cudaEventCreate(&x.end) != cudaSuccess ||
-        cudaEventRecord(x.start, c->stream) != cudaSuccess) {
+        cudaEventRecord(x.start, stream) != cudaSuccess) {
         if (x.start) cudaEventDestroy(x.start);
         if (x.end) cudaEventDestroy(x.end);
         cudaGetLastError();
@@ -67,7 +67,7 @@ GpuPass::GpuPass(ol_ctx *c, const char *label) : ctx(c) {
 
 void GpuPass::done() {
     if (index < 0 || !ctx->prof || index >= (int)ctx->prof->passes.size()) return;
-    if (cudaEventRecord(ctx->prof->passes[index].end, ctx->stream) != cudaSuccess) cudaGetLastError();
+    if (cudaEventRecord(ctx->prof->passes[index].end, stream) != cudaSuccess) cudaGetLastError();
     index = -1;
 }
 

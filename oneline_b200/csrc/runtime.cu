@@ -106,6 +106,11 @@ extern "C" ol_status ol_ctx_create(int32_t device, ol_ctx **out) {
         delete c;
         return OL_ERR_CUDA;
     }
+    if ((e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->copy_ready, cudaEventDisableTiming)) != cudaSuccess) {
+        ol_ctx_destroy(c);
+        return OL_ERR_CUDA;
+    }
     // Keep freed pool memory around: documents come and go.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -156,6 +161,10 @@ extern "C" void ol_ctx_destroy(ol_ctx *ctx) {
         if (ctx->ring_done[i]) cudaEventDestroy(ctx->ring_done[i]);
     }
     prof_discard(ctx);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    for (cudaEvent_t ev : ctx->chunk_done) cudaEventDestroy(ev);
+    if (ctx->copy_ready) cudaEventDestroy(ctx->copy_ready);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -210,15 +219,15 @@ cudaError_t h2d(ol_ctx *ctx, uint8_t *dev, const uint8_t *host, uint64_t len) {
     return cudaSuccess;
 }
 
-// Enqueues the parse of doc's resident text into its buffers.
-cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d) {
-    GpuPass pass(ctx, "parse");
+// The staged parse's arguments for doc, with the context's scratch reserved
+// and the document's counters reset (enqueued on the context stream).
+static cudaError_t parse_args(ol_ctx *ctx, ol_doc *d, ParseArgs &a) {
     cudaStream_t st = ctx->stream;
     cudaError_t e;
     uint32_t n_tiles = parse_tiles(d->text_len);
     if ((e = ctx->scratch_a.reserve((size_t)scan_ld(n_tiles) * 8, st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(d->stats, 0, sizeof(DocStats), st)) != cudaSuccess) return e;
-    ParseArgs a{};
+    a = ParseArgs{};
     a.text = d->text;
     a.text_len = d->text_len;
     a.n_tiles = n_tiles;
@@ -241,7 +250,72 @@ cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d) {
     a.redo_n = (uint32_t *)(ps + list_at);
     a.redo_list = a.redo_n + 4;
     a.slot_cap = kParseSlotCap;
-    return launch_parse(a, st);
+    return cudaSuccess;
+}
+
+// Enqueues the parse of doc's resident text into its buffers.
+cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d) {
+    GpuPass pass(ctx, "parse");
+    ParseArgs a;
+    cudaError_t e = parse_args(ctx, d, a);
+    return e == cudaSuccess ? launch_parse(a, ctx->stream) : e;
+}
+
+// The upload chunk after which the stage pass runs on the tiles that have
+// arrived (a 16 MiB ring slot for pageable text).
+constexpr uint64_t kOverlapChunk = 32ull << 20;
+constexpr size_t kMaxChunksInFlight = 64;
+
+cudaError_t upload_parse_overlapped(ol_ctx *ctx, ol_doc *d, const uint8_t *host, uint64_t len) {
+    cudaStream_t st = ctx->stream, cs = ctx->copy_stream;
+    cudaError_t e;
+    while (ctx->chunk_done.size() < kMaxChunksInFlight) {
+        cudaEvent_t ev;
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+        ctx->chunk_done.push_back(ev);
+    }
+    GpuPass parse_pass(ctx, "parse (overlapped with the upload)");
+    ParseArgs a;
+    if ((e = parse_args(ctx, d, a)) != cudaSuccess) return e;
+    if ((e = launch_parse_begin(a, st)) != cudaSuccess) return e;
+    // the copies start after the document's buffers exist on the main stream
+    if ((e = cudaEventRecord(ctx->copy_ready, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(cs, ctx->copy_ready, 0)) != cudaSuccess) return e;
+    cudaPointerAttributes attr;
+    const bool pinned = cudaPointerGetAttributes(&attr, host) == cudaSuccess &&
+                        (attr.type == cudaMemoryTypeHost || attr.type == cudaMemoryTypeManaged);
+    cudaGetLastError();
+    const uint64_t chunk = pinned ? std::max<uint64_t>(kOverlapChunk, (len + kMaxChunksInFlight - 1) / kMaxChunksInFlight)
+                                  : kRingBytes;
+    GpuPass copy_pass(ctx, "upload: copy to device", cs);
+    uint32_t t0 = 0;
+    for (uint64_t off = 0, i = 0; off < len; off += chunk, i++) {
+        const uint64_t n = std::min<uint64_t>(chunk, len - off);
+        cudaEvent_t landed;
+        if (pinned) {
+            landed = ctx->chunk_done[i % kMaxChunksInFlight];
+            if ((e = cudaMemcpyAsync(d->text + off, host + off, n, cudaMemcpyHostToDevice, cs)) != cudaSuccess) return e;
+        } else {
+            const int slot = (int)(i % kRingSlots);  // the ring: the copy of chunk i+1 into a pinned slot
+            landed = ctx->ring_done[slot];            // overlaps the DMA of chunk i (staging.rs:59-117)
+            if ((e = cudaEventSynchronize(landed)) != cudaSuccess) return e;
+            memcpy(ctx->ring[slot], host + off, n);
+            if ((e = cudaMemcpyAsync(d->text + off, ctx->ring[slot], n, cudaMemcpyHostToDevice, cs)) != cudaSuccess)
+                return e;
+        }
+        if ((e = cudaEventRecord(landed, cs)) != cudaSuccess) return e;
+        // tiles whose bytes and halo have landed: (t + 1) * tile + halo <= off + n
+        const uint64_t have = off + n;
+        const uint32_t t1 = have == len ? a.n_tiles
+                                        : (uint32_t)(have >= kParseHalo ? (have - kParseHalo) / kParseTile : 0);
+        if (t1 > t0) {
+            if ((e = cudaStreamWaitEvent(st, landed, 0)) != cudaSuccess) return e;
+            if ((e = launch_parse_tiles(a, t0, t1, st)) != cudaSuccess) return e;
+            t0 = t1;
+        }
+    }
+    copy_pass.done();
+    return launch_parse_end(a, st);
 }
 
 ol_status alloc_lines(ol_ctx *ctx, ol_doc *d, uint64_t cap_lines) {
@@ -264,12 +338,14 @@ ol_status alloc_lines(ol_ctx *ctx, ol_doc *d, uint64_t cap_lines) {
 // Runs the parse (with one exact-size retry when the estimate was too low),
 // waits, and records the line count. With nodes_out, the 16-byte nodes are
 // materialised into ctx->scratch_c as well.
-ol_status parse_doc(ol_ctx *ctx, ol_doc *d, uint64_t est_lines, FlatNode **nodes_out) {
+ol_status parse_doc(ol_ctx *ctx, ol_doc *d, uint64_t est_lines, FlatNode **nodes_out, const uint8_t *host_text) {
     cudaStream_t st = ctx->stream;
     for (int attempt = 0; attempt < 2; attempt++) {
         ol_status s = alloc_lines(ctx, d, est_lines);
         if (s != OL_OK) return s;
-        cudaError_t e = enqueue_parse(ctx, d);
+        // the first attempt uploads the text as it parses; a retry finds it resident
+        cudaError_t e = attempt == 0 && host_text ? upload_parse_overlapped(ctx, d, host_text, d->text_len)
+                                                  : enqueue_parse(ctx, d);
         if (e == cudaSuccess) e = cudaMemcpyAsync(&d->host_stats, d->stats, sizeof(DocStats), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return ctx_cuda(ctx, e, "parse");
@@ -343,15 +419,14 @@ static ol_status upload_common(ol_ctx *ctx, const uint8_t *text, uint64_t len, b
         e = cudaMemcpyAsync(d->text, text, len, cudaMemcpyDeviceToDevice, ctx->stream);
         est = len / 24 + 4096;  // no host copy to sample; a low guess costs one retry
     } else {
-        e = h2d(ctx, d->text, text, len);
         est = estimate_lines(text, len);
+        e = cudaSuccess;
     }
-    prof_mark(ctx, "upload: enqueue copy");
     if (e != cudaSuccess) {
         ol_doc_free(d);
         return ctx_cuda(ctx, e, "upload");
     }
-    s = parse_doc(ctx, d, est, nullptr);
+    s = parse_doc(ctx, d, est, nullptr, device_src ? nullptr : text);
     prof_mark(ctx, "upload: wait for parse");
     if (s != OL_OK) {
         ol_doc_free(d);
@@ -458,10 +533,9 @@ extern "C" ol_status ol_parse_raw(ol_ctx *ctx, const uint8_t *text, uint64_t len
         s = new_doc(ctx, len, &d);
         if (s != OL_OK) return s;
         if (len > 0) {
-            cudaError_t e = h2d(ctx, d->text, text, len);
-            if (e != cudaSuccess) s = ctx_cuda(ctx, e, "upload");
+            cudaError_t e = cudaSuccess;
             FlatNode *dn = nullptr;
-            if (s == OL_OK) s = parse_doc(ctx, d, estimate_lines(text, len), nodes ? &dn : nullptr);
+            s = parse_doc(ctx, d, estimate_lines(text, len), nodes ? &dn : nullptr, text);  // upload overlapped
             *line_count = d->line_count;
             if (s == OL_OK && d->line_count <= cap && d->line_count > 0) {
                 cudaStream_t st = ctx->stream;

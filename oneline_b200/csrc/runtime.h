@@ -52,6 +52,9 @@ struct ol_ctx {
     uint64_t dict_stats[6] = {0, 0, 0, 0, 0, 0};  // the last dictionary search (ol_dict_stats)
     uint32_t inject = 0;  // OL_INJECT_* faults armed for the next operation they name (ol_ctx_inject)
     ol::Prof *prof = nullptr;  // open profile (ol_profile_begin), or null
+    cudaStream_t copy_stream = nullptr;  // uploads that overlap the parse
+    cudaEvent_t copy_ready = nullptr;    // the main stream's work before an upload
+    std::vector<cudaEvent_t> chunk_done; // one per upload chunk in flight
     ol::DevBuf pattern_dev;
     ol::DevBuf dict_small;   // dictionary search: per-pattern counts, ranks, slots
     ol::DevBuf dict_bitmap;  // heavy-pattern bitmaps
@@ -96,8 +99,10 @@ namespace ol {
 // prof_mark ends a host step.
 struct GpuPass {
     ol_ctx *ctx;
+    cudaStream_t stream;
     int index = -1;
-    GpuPass(ol_ctx *c, const char *label);
+    GpuPass(ol_ctx *c, const char *label) : GpuPass(c, label, nullptr) {}
+    GpuPass(ol_ctx *c, const char *label, cudaStream_t on);  // on: a stream of ctx (null: its main stream)
     ~GpuPass() { done(); }
     void done();  // ends the pass here instead of at destruction
     GpuPass(const GpuPass &) = delete;
@@ -112,8 +117,15 @@ uint32_t parse_tiles(uint64_t len);
 uint32_t round_lines(uint64_t n);
 ol_status new_text_doc(ol_ctx *ctx, const uint8_t *text, uint64_t len, ol_doc **out);
 ol_status new_doc(ol_ctx *ctx, uint64_t len, ol_doc **out);
-ol_status parse_doc(ol_ctx *ctx, ol_doc *d, uint64_t est_lines, FlatNode **nodes_out);
+// Parses doc's text and waits (one retry with the exact line count when the
+// estimate was low). With host_text, the text is uploaded first, overlapped
+// with the parse.
+ol_status parse_doc(ol_ctx *ctx, ol_doc *d, uint64_t est_lines, FlatNode **nodes_out,
+                    const uint8_t *host_text = nullptr);
 cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d);
+// Uploads host text into doc (allocated, line arrays reserved) and parses it,
+// the copy of each chunk overlapping the stage pass of the chunks before it.
+cudaError_t upload_parse_overlapped(ol_ctx *ctx, ol_doc *d, const uint8_t *host, uint64_t len);
 cudaError_t enqueue_tree(ol_ctx *ctx, const ol_doc *d, ol_tree *t);
 cudaError_t launch_multi(ol_ctx *ctx, const ol_doc *d, const uint8_t *const *hpats, const uint8_t *const *dpats,
                          const uint32_t *lens, uint32_t n, const uint32_t *max_out, uint32_t *d_totals,

@@ -123,3 +123,27 @@ def test_reparse_into_the_same_buffers(parser):
     parser.sync()
     assert np.array_equal(doc.read_nodes(), before)
     assert np.array_equal(doc.read_offsets(), oracle.scan_line_offsets(text))
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_upload_overlapped_with_the_parse_across_chunks(parser, pinned):
+    """The upload streams the text in chunks (16 MiB ring slots for pageable
+    memory, 32 MiB copies for pinned) and the parse runs on each chunk's tiles
+    as they land: lines and long lines that straddle chunk edges, and a text
+    that ends right after a chunk edge, parse as they do in one piece."""
+    import torch
+
+    base = datagen.corpus((70 << 20) + 5, 23).tobytes()
+    long_line = b"|| - " + b"x" * 70_000 + b"\n"
+    edge = 16 << 20
+    text = base[: edge - 30_000] + long_line + base[edge - 30_000: 3 * (32 << 20) + 7]
+    for t in (text, text[: 2 * (16 << 20) + 1]):
+        want_offs, want_nodes = oracle.CpuBaseline().parse_par(t)
+        src = t
+        if pinned:
+            h = torch.empty(len(t), dtype=torch.uint8, pin_memory=True)
+            h.numpy()[:] = np.frombuffer(t, np.uint8)
+            src = h.numpy()
+        doc = parser.upload(src)
+        assert np.array_equal(doc.read_offsets(), want_offs)
+        assert np.array_equal(doc.read_nodes(), want_nodes)

@@ -31,7 +31,7 @@ def test_profile_upload_search_tree_and_queries(parser):
     text = datagen.corpus(4 << 20, 31).tobytes()
     doc, prof = parser.profile_upload(text)
     check_profile(prof)
-    assert {"upload: copy to device", "parse"} <= set(labels(prof))
+    assert {"upload: copy to device", "parse (overlapped with the upload)"} <= set(labels(prof))
     assert labels(prof, "host_steps")[-1] == "upload: wait for parse"
     offs, nodes = oracle.parse(text)
     assert np.array_equal(doc.read_offsets(), offs)
