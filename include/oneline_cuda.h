@@ -148,6 +148,21 @@ ol_status ol_doc_read_nodes(ol_ctx *ctx, const ol_doc *doc, ol_flat_node *out, u
 ol_status ol_doc_device_views(const ol_doc *doc, const uint8_t **text, const uint32_t **offsets, const uint8_t **kinds,
                               const uint8_t **depth8);
 
+/* ---- the .olb binary format: FlatTree::save_to_file / open_mmap as planned in
+ *      .agents/tasks/phase4-zero-copy-binary-serialization.md:13-36 (64-byte
+ *      header "ONELINE\0", version 1, text_len, line_count, section offsets,
+ *      CRC-32; then the text, FlatNode[line_count] and u32 line offsets, each
+ *      section on a 64-byte boundary). ol_doc_save_olb writes a resident
+ *      document's text, nodes and offsets. ol_doc_load_olb maps a file and
+ *      makes it a resident document without parsing: the text, offsets and
+ *      nodes are copied to the device (by DMA from the mapped pages where they
+ *      can be registered) and the kinds and depths come from the nodes. A file
+ *      whose header, sections or offsets do not hold together is refused with
+ *      OL_ERR_INVALID_ARG; with OL_OLB_VERIFY its checksum is checked too. */
+#define OL_OLB_VERIFY 1u
+ol_status ol_doc_save_olb(ol_ctx *ctx, const ol_doc *doc, const char *path);
+ol_status ol_doc_load_olb(ol_ctx *ctx, const char *path, uint32_t flags, ol_doc **out);
+
 /* ---- one-shot parse: GpuParser::parse_raw, scan_line_offsets, parse(input, offsets)
  *      (crates/oneline-gpu/src/parse.rs:86-125, scan.rs:127-136). *line_count
  *      always receives the true count; outputs are written when cap allows. */

@@ -50,6 +50,8 @@ SIGNATURES: dict[str, tuple] = {
     "ol_doc_read_kinds": (_S, [_P, _P, _P, _U64]),
     "ol_doc_read_nodes": (_S, [_P, _P, _P, _U64]),
     "ol_doc_device_views": (_S, [_P, _PP, _PP, _PP, _PP]),
+    "ol_doc_save_olb": (_S, [_P, _P, ctypes.c_char_p]),
+    "ol_doc_load_olb": (_S, [_P, ctypes.c_char_p, _U32, _PP]),
     "ol_parse_raw": (_S, [_P, _U8P, _U64, _P, _P, _U64, _U64P]),
     "ol_scan_line_offsets": (_S, [_P, _U8P, _U64, _P, _U64, _U64P]),
     "ol_parse_with_offsets": (_S, [_P, _U8P, _U64, _P, _U64, _P]),

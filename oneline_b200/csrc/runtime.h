@@ -123,6 +123,9 @@ ol_status new_doc(ol_ctx *ctx, uint64_t len, ol_doc **out);
 ol_status parse_doc(ol_ctx *ctx, ol_doc *d, uint64_t est_lines, FlatNode **nodes_out,
                     const uint8_t *host_text = nullptr);
 cudaError_t enqueue_parse(ol_ctx *ctx, ol_doc *d);
+// Copies host bytes to device memory on the context stream (pinned: one DMA;
+// pageable: through the pinned staging ring).
+cudaError_t h2d(ol_ctx *ctx, uint8_t *dev, const uint8_t *host, uint64_t len);
 // Uploads host text into doc (allocated, line arrays reserved) and parses it,
 // the copy of each chunk overlapping the stage pass of the chunks before it.
 cudaError_t upload_parse_overlapped(ol_ctx *ctx, ol_doc *d, const uint8_t *host, uint64_t len);

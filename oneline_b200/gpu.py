@@ -460,6 +460,19 @@ class GpuParser:
         """parent, subtree_end, first_child and next_sibling of every line."""
         return self._read_tree(tree, ("parent", "subtree_end", "first_child", "next_sibling"))
 
+    # ------------------------------------------------------------ .olb files
+
+    def save_olb(self, doc: GpuDocument, path: str) -> None:
+        """Writes the resident document's text, nodes and line offsets as an .olb file."""
+        check(_lib.load().ol_doc_save_olb(self._ctx, doc.handle, path.encode()), self._ctx)
+
+    def load_olb(self, path: str, *, verify: bool = False) -> GpuDocument:
+        """A resident document from an .olb file, without parsing its text
+        (``verify`` also checks the file's CRC-32)."""
+        h = ctypes.c_void_p()
+        check(_lib.load().ol_doc_load_olb(self._ctx, path.encode(), 1 if verify else 0, ctypes.byref(h)), self._ctx)
+        return GpuDocument(self, h.value, path)
+
     # --------------------------------------------------------------- search
 
     @staticmethod
