@@ -634,12 +634,22 @@ def run_ours(args, world, rank, local):
     if not args.no_graph:
         pipe.free()
     del outs
+    def sub_record(fn, *a):
+        # a sub-record that fails is reported as such; the headline line stands
+        try:
+            return fn(*a)
+        except Exception as e:  # noqa: BLE001
+            import traceback
+
+            traceback.print_exc()
+            return {"error": f"{type(e).__name__}: {e}"[:300]}
+
     if world == 1 and not args.no_dictionary:
-        dict_rec = dictionary_record(args, world, rank, local, p)
+        dict_rec = sub_record(dictionary_record, args, world, rank, local, p)
     if world == 1 and not args.no_batch:
-        batch_rec = batch_record(args, world, rank, local, p)
+        batch_rec = sub_record(batch_record, args, world, rank, local, p)
     if world == 1 and not args.no_serve:
-        serve_rec = serve_record(args, local)
+        serve_rec = sub_record(serve_record, args, local)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
