@@ -423,348 +423,116 @@ __global__ void __launch_bounds__(SR_THREADS) search_write_kernel(SearchArgs a) 
 // ----------------------------------------------------------- staged path --
 //
 // With a staging buffer the filter and verification run once: pass 1
-// (search_stage_kernel) finds each tile's matches, counts every pattern's hits
-// with one block scan for all patterns at once, and writes the tile's hits, in
-// (pattern, position) order, as 16-bit tile offsets into the tile's staging
-// slot. After the column scan, pass 2 (search_copy_kernel) copies them to their
-// final slots. A tile with more hits than its staging slot holds is flagged and
-// left to search_write_kernel, which recomputes it.
-//
-// search_stage_kernel keeps the text in registers: thread t of a block owns
-// the 64 bytes [64t, 64t + 64) of its tile (four 16-byte pieces), loaded with
-// four 16-byte loads, plus the word after them (from the next lane). Its match
-// masks stay in registers, one 64-bit mask per pattern (bit i = byte 64t + i),
-// so the epilogue scans them without a shared-memory transpose. Candidate
-// pieces of patterns over 4 bytes are verified from global memory (the L1/L2
-// copy of the tile just read); their masks reach the owning lane through a
-// per-warp shared area, zeroed only in warps that queue a candidate. Blocks
-// are persistent: the pattern table and the anchor map are built once per
-// block, then the block takes tiles b, b + grid, b + 2 grid, ...
-
-constexpr uint32_t SS_THREADS = 256;
-constexpr uint32_t SS_WARPS = SS_THREADS / 32;
-constexpr uint32_t kAnchorMapBits = 13;  // byte map of anchor-word hashes (8 KiB)
-static_assert(SS_THREADS * 64 == kSearchTile, "a thread owns 64 bytes of the tile");
-
-__host__ __device__ __forceinline__ uint32_t anchor_hash13(uint32_t w) { return (w * 0x9E3779B1u) >> (32 - kAnchorMapBits); }
+// (search_stage_kernel) keeps each tile's match masks in shared memory, counts
+// every pattern's hits with one block scan for all patterns at once, and writes
+// the tile's hits, in (pattern, position) order, as 16-bit tile offsets into the
+// tile's staging slot. After the column scan, pass 2 (search_copy_kernel)
+// copies them to their final slots. A tile with more hits than its staging slot
+// holds is flagged and left to search_write_kernel, which recomputes it.
 
 template <uint32_t NP>
-struct StageSmem {
-    uint8_t amap[1u << kAnchorMapBits];  // 1 where some anchor word of the launch hashes
-    union {
-        uint32_t vres[SS_WARPS][NP][32][2];     // verified masks of patterns over 4 bytes, by owner lane
-        uint16_t stage[kSearchStageCap];       // the tile's hits in (pattern, position) order
-    } u;
-    uint16_t queue[SS_WARPS][SR_QCAP];       // (pattern << 10) | piece, per warp
-    uint32_t wsum[SS_WARPS][(NP + 1) / 2];   // per-warp totals of the packed counts
-    uint32_t wact[SS_WARPS];                 // per-warp patterns with hits
-    PatMeta pat[NP];
-};
-
-// Bytes [q, q + 16) of the text (bytes at or past N read as 0).
-__device__ __forceinline__ uint4 gwin16(const uint8_t *text, uint64_t q, uint64_t N) {
-    if (q + 20 <= N) {
-        const uint32_t *w = reinterpret_cast<const uint32_t *>(text + (q & ~3ull));
-        const uint32_t sh = (uint32_t)(q & 3) * 8;
-        const uint32_t a0 = __ldg(w), a1 = __ldg(w + 1), a2 = __ldg(w + 2), a3 = __ldg(w + 3), a4 = __ldg(w + 4);
-        return make_uint4(__funnelshift_r(a0, a1, sh), __funnelshift_r(a1, a2, sh), __funnelshift_r(a2, a3, sh),
-                          __funnelshift_r(a3, a4, sh));
-    }
-    uint8_t b[16];
-#pragma unroll
-    for (int r = 0; r < 16; r++) b[r] = q + r < N ? __ldg(text + q + r) : (uint8_t)0;
-    return *reinterpret_cast<uint4 *>(b);
-}
-
-// Exact matches of a pattern at the sixteen starts of the piece at tile-local
-// byte lo, read from global memory: the first byte, the last, then the others,
-// all sixteen starts at once, stopping when none is left.
-__device__ __forceinline__ uint32_t verify_piece_global(const SearchArgs &a, const PatMeta &pm, uint64_t t0, uint32_t lo,
-                                                        bool tail_tile) {
-    const uint32_t m = pm.len;
-    const uint4 v = gwin16(a.text, t0 + lo, a.text_len);
-    uint32_t c0 = zero_bytes(v.x ^ pm.f4), c1 = zero_bytes(v.y ^ pm.f4);
-    uint32_t c2 = zero_bytes(v.z ^ pm.f4), c3 = zero_bytes(v.w ^ pm.f4);
-    if (tail_tile) keep_valid_starts(a.text_len, m, t0, lo, c0, c1, c2, c3);
-    for (uint32_t jj = 1; jj < m && (c0 | c1 | c2 | c3); jj++) {
-        const uint32_t j = jj == 1 ? m - 1 : jj - 1;  // last byte first, then 1, 2, ...
-        const uint32_t P4 = __ldg(pm.ptr + j) * 0x01010101u;
-        const uint4 w = gwin16(a.text, t0 + lo + j, a.text_len);
-        c0 &= zero_bytes(w.x ^ P4);
-        c1 &= zero_bytes(w.y ^ P4);
-        c2 &= zero_bytes(w.z ^ P4);
-        c3 &= zero_bytes(w.w ^ P4);
-    }
-    return gather16(c0, c1, c2, c3);
-}
-
-template <uint32_t NP>
-__global__ void __launch_bounds__(SS_THREADS, 4) search_stage_kernel(SearchArgs a) {
+__global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) {
     constexpr uint32_t NQ = (NP + 1) / 2;  // packed count words, two patterns each
-    __shared__ StageSmem<NP> sm;
+    __shared__ SearchSmem sm;
+    __shared__ uint16_t match[NP][SR_PIECES];
+    __shared__ uint32_t warp_sum[SR_THREADS / 32][NQ];
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-
-    // Once per block: the pattern table and the anchor map.
-    for (uint32_t o = tid; o < (1u << kAnchorMapBits) / 16; o += SS_THREADS)
-        reinterpret_cast<uint4 *>(sm.amap)[o] = make_uint4(0, 0, 0, 0);
+    const uint32_t tile = blockIdx.x;
+    const uint64_t t0 = (uint64_t)tile * kSearchTile;
+    load_tile(a, sm, t0);
+    if (tid == 0) sm.active = 0;
+    for (uint32_t o = tid; o < NP * SR_PIECES / 8; o += SR_THREADS)
+        reinterpret_cast<uint4 *>(&match[0][0])[o] = make_uint4(0, 0, 0, 0);
     __syncthreads();
-    if (tid < NP) {
-        const SearchPatMeta &m = a.meta[tid];
-        PatMeta pm;
-        pm.ptr = a.pat[tid];
-        pm.len = m.len;
-        pm.f4 = m.f4;
-        pm.pre = make_uint4(m.pre[0], m.pre[1], m.pre[2], m.pre[3]);
-        pm.anc = make_uint4(m.anc[0], m.anc[1], m.anc[2], m.anc[3]);
-        sm.pat[tid] = pm;
-        if (m.len >= kAnchorMin)
-            for (int r = 0; r < 4; r++) sm.amap[anchor_hash13(m.anc[r])] = 1;  // byte stores: no atomics needed
-    }
+    filter_tile<NP>(a, sm, (1u << NP) - 1u, t0,
+                    [&](uint32_t p, uint32_t piece, uint32_t mk) { match[p][piece] = (uint16_t)mk; });
     __syncthreads();
-    uint32_t shorts = 0, mids = 0, anchored = 0;  // patterns by length: <= 4, 5-7, >= 8
+    // my hits per pattern (4 pieces: at most 64), and the patterns with hits
+    // anywhere in the tile: a tile without hits is done here
+    uint2 m4[NP];
+    uint32_t mine_any = 0;
 #pragma unroll
     for (uint32_t p = 0; p < NP; p++) {
-        const uint32_t m = sm.pat[p].len;
-        if (m <= 4) shorts |= 1u << p;
-        else if (m < kAnchorMin) mids |= 1u << p;
-        else anchored |= 1u << p;
+        m4[p] = *reinterpret_cast<const uint2 *>(&match[p][4 * tid]);
+        mine_any |= (m4[p].x | m4[p].y) ? 1u << p : 0u;
     }
-    const uint32_t longs = mids | anchored;
-    uint16_t *queue = sm.queue[warp];
-
-    for (uint32_t tile = blockIdx.x; tile < a.n_tiles; tile += gridDim.x) {
-        const uint64_t t0 = (uint64_t)tile * kSearchTile;
-        // a match starting in a tail tile may end past the text (zero padding)
-        const bool tail_tile = t0 + kSearchTile + a.halo + 32 > a.text_len;
-        const uint8_t *src = a.text + t0 + 64 * tid;
-        // the thread's 64 bytes, then the word after them (the next lane's first)
-        uint32_t w[17];
-        {
-            const uint4 v0 = ld_stream16(src), v1 = ld_stream16(src + 16), v2 = ld_stream16(src + 32),
-                        v3 = ld_stream16(src + 48);
-            w[0] = v0.x; w[1] = v0.y; w[2] = v0.z; w[3] = v0.w;
-            w[4] = v1.x; w[5] = v1.y; w[6] = v1.z; w[7] = v1.w;
-            w[8] = v2.x; w[9] = v2.y; w[10] = v2.z; w[11] = v2.w;
-            w[12] = v3.x; w[13] = v3.y; w[14] = v3.z; w[15] = v3.w;
-        }
-        w[16] = __shfl_down_sync(0xFFFFFFFFu, w[0], 1);
-        if (lane == 31) w[16] = __ldg(reinterpret_cast<const uint32_t *>(src + 64));
-
-        // Filter, piece by piece (the loop is rolled: the window of five words
-        // moves down the registers). m[p]: bit 16j + i = a match at byte 16j + i
-        // of the thread's span, shifted in from the top one piece per step.
-        unsigned long long m[NP];
-#pragma unroll
-        for (uint32_t p = 0; p < NP; p++) m[p] = 0;
-        uint32_t cand = 0;  // bit 4p + j: piece j has a candidate of pattern p
-#pragma unroll 1
-        for (uint32_t j = 0; j < 4; j++) {
-            const uint32_t lo = 64 * tid + 16 * j;
-            uint32_t s1[4], s2[4], s3[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) s1[i] = __funnelshift_r(w[i], w[i + 1], 8);
-            if (shorts) {  // uniform
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    s2[i] = __funnelshift_r(w[i], w[i + 1], 16);
-                    s3[i] = __funnelshift_r(w[i], w[i + 1], 24);
-                }
-            }
-#pragma unroll
-            for (uint32_t p = 0; p < NP; p++) {
-                uint32_t mk = 0;
-                if ((shorts >> p) & 1u) {  // uniform
-                    const uint4 pre = sm.pat[p].pre;
-                    const uint32_t ml = sm.pat[p].len;
-                    uint32_t x[4];
-#pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        x[i] = w[i] ^ pre.x;
-                        if (ml > 1) x[i] |= s1[i] ^ pre.y;
-                        if (ml > 2) x[i] |= s2[i] ^ pre.z;
-                        if (ml > 3) x[i] |= s3[i] ^ pre.w;
-                    }
-                    uint32_t c0 = zero_bytes(x[0]), c1 = zero_bytes(x[1]), c2 = zero_bytes(x[2]), c3 = zero_bytes(x[3]);
-                    if (tail_tile) keep_valid_starts(a.text_len, ml, t0, lo, c0, c1, c2, c3);
-                    if (c0 | c1 | c2 | c3) mk = gather16(c0, c1, c2, c3);
-                } else if ((mids >> p) & 1u) {  // the first two bytes (loose SWAR; exact as "any")
-                    const uint4 pre = sm.pat[p].pre;
-                    uint32_t acc = 0;
-#pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        const uint32_t x = (w[i] ^ pre.x) | (s1[i] ^ pre.y);
-                        acc |= (x - 0x01010101u) & ~x;
-                    }
-                    cand |= (uint32_t)((acc & 0x80808080u) != 0) << (4 * p + j);
-                }
-                m[p] = (m[p] >> 16) | ((unsigned long long)mk << 48);
-            }
-            if (anchored) {  // uniform
-                // the four aligned words that anchor the piece's sixteen starts:
-                // w[i] anchors the starts 16j + 4i - 4 .. 16j + 4i - 1 (i = 1..4)
-                uint32_t hit = 0;
-#pragma unroll
-                for (int i = 1; i < 5; i++) hit |= sm.amap[anchor_hash13(w[i])];
-                if (hit) {  // rare: compare the anchors exactly
-#pragma unroll
-                    for (uint32_t p = 0; p < NP; p++) {
-                        if (!((anchored >> p) & 1u)) continue;
-                        const uint4 c = sm.pat[p].anc;
-                        bool any = false;
-#pragma unroll
-                        for (int i = 1; i < 5; i++) any |= w[i] == c.x || w[i] == c.y || w[i] == c.z || w[i] == c.w;
-                        cand |= (uint32_t)any << (4 * p + j);
-                    }
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < 13; i++) w[i] = w[i + 4];
-        }
-
-        // Candidates of the longer patterns: queued per warp, verified 32 at a
-        // time (one per lane), and their masks or'ed into the owner lane's slot.
-        if (longs && __any_sync(0xFFFFFFFFu, cand != 0)) {  // uniform
-            uint32_t(*vres)[32][2] = sm.u.vres[warp];
-            for (uint32_t o = lane; o < NP * 64; o += 32) (&vres[0][0][0])[o] = 0;
-            __syncwarp();
-            uint32_t qn = 0;
-            auto drain = [&](uint32_t n) {
-                for (uint32_t done = 0; done < n; done += 32) {
-                    if (done + lane < n) {
-                        const uint32_t e = queue[done + lane];
-                        const uint32_t p = e >> 10, piece = e & 1023u;
-                        const uint32_t mk = verify_piece_global(a, sm.pat[p], t0, piece * 16, tail_tile);
-                        if (mk) atomicOr(&vres[p][(piece >> 2) & 31][(piece >> 1) & 1], mk << (16 * (piece & 1)));
-                    }
-                }
-            };
-#pragma unroll
-            for (uint32_t p = 0; p < NP; p++) {
-                if (!((longs >> p) & 1u)) continue;
-                uint32_t cm = (cand >> (4 * p)) & 0xFu;
-                if (!__any_sync(0xFFFFFFFFu, cm != 0)) continue;
-                const uint32_t n = __popc(cm);
-                uint32_t inc = n;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
-                    if ((int)lane >= o) inc += t;
-                }
-                uint32_t pos = qn + inc - n;
-                while (cm) {
-                    const uint32_t j = __ffs(cm) - 1;
-                    cm &= cm - 1;
-                    queue[pos++] = (uint16_t)((p << 10) | (4 * tid + j));
-                }
-                qn += __shfl_sync(0xFFFFFFFFu, inc, 31);
-                __syncwarp();
-                if (qn >= 32) {
-                    const uint32_t full = qn & ~31u;
-                    drain(full);
-                    const uint32_t rem = qn - full;
-                    const uint16_t keep = lane < rem ? queue[full + lane] : (uint16_t)0;
-                    __syncwarp();
-                    if (lane < rem) queue[lane] = keep;
-                    qn = rem;
-                    __syncwarp();
-                }
-            }
-            drain(qn);
-            __syncwarp();
-#pragma unroll
-            for (uint32_t p = 0; p < NP; p++)
-                if ((longs >> p) & 1u)
-                    m[p] |= (unsigned long long)vres[p][lane][0] | ((unsigned long long)vres[p][lane][1] << 32);
-        }
-
-        // Counts, two patterns per word (a thread has at most 64 hits of a
-        // pattern, a tile at most 16384: 16 bits each), inclusive warp scans of
-        // the words that hold a pattern with hits in this warp.
-        uint32_t mine_any = 0;
-#pragma unroll
-        for (uint32_t p = 0; p < NP; p++) mine_any |= m[p] ? 1u << p : 0u;
-        const uint32_t wact = __reduce_or_sync(0xFFFFFFFFu, mine_any);
-        uint32_t packed[NQ], inc[NQ];
-#pragma unroll
-        for (uint32_t q = 0; q < NQ; q++) packed[q] = 0;
-#pragma unroll
-        for (uint32_t p = 0; p < NP; p++) packed[p >> 1] |= (uint32_t)__popcll(m[p]) << (16 * (p & 1));
-#pragma unroll
-        for (uint32_t q = 0; q < NQ; q++) {
-            inc[q] = packed[q];
-            if ((wact >> (2 * q)) & 3u) {  // uniform
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc[q], o);
-                    if ((int)lane >= o) inc[q] += t;
-                }
-            }
-            if (lane == 31) sm.wsum[warp][q] = inc[q];
-        }
-        if (lane == 0) sm.wact[warp] = wact;
-        __syncthreads();  // (a) warp totals; every warp's vres has been read
-        uint32_t active = 0;
-#pragma unroll
-        for (uint32_t x = 0; x < SS_WARPS; x++) active |= sm.wact[x];
-        uint32_t before[NQ], total[NQ];
-#pragma unroll
-        for (uint32_t q = 0; q < NQ; q++) {
-            before[q] = total[q] = 0;
-            if ((active >> (2 * q)) & 3u)
-#pragma unroll
-                for (uint32_t x = 0; x < SS_WARPS; x++) {
-                    const uint32_t v = sm.wsum[x][q];
-                    before[q] += x < warp ? v : 0u;
-                    total[q] += v;
-                }
-        }
-        uint32_t start = 0;
-        uint32_t tot_p = 0;  // thread p < NP: pattern p's tile total
-#pragma unroll
-        for (uint32_t p = 0; p < NP; p++) {
-            const uint32_t tot = (total[p >> 1] >> (16 * (p & 1))) & 0xFFFFu;
-            if (tid == p) tot_p = tot;
-            start += tot;
-        }
-        const bool over = start > a.stage_cap;
-        if (tid < NP) a.counts[(size_t)tid * a.ld + tile] = tot_p;
-        if (tid == 0) {
-            a.overflow[tile] = over ? 1 : 0;
-            if (over) a.overflow_list[atomicAdd(a.overflow_n, 1u)] = tile;
-        }
-        if (active && !over) {  // uniform
-            // each thread writes its hits at its rank in the tile's (pattern,
-            // position) order; the slot is assembled in shared memory and stored
-            // with 16-byte writes
-            uint32_t at = 0;
-#pragma unroll
-            for (uint32_t p = 0; p < NP; p++) {
-                const uint32_t sh = 16 * (p & 1);
-                const uint32_t tot = (total[p >> 1] >> sh) & 0xFFFFu;
-                if ((active >> p) & 1u) {
-                    const uint32_t mine = (packed[p >> 1] >> sh) & 0xFFFFu;
-                    uint32_t r = at + ((before[p >> 1] >> sh) & 0xFFFFu) + ((inc[p >> 1] >> sh) & 0xFFFFu) - mine;
-                    const uint32_t mm[2] = {(uint32_t)m[p], (uint32_t)(m[p] >> 32)};
-#pragma unroll
-                    for (uint32_t h = 0; h < 2; h++) {
-                        uint32_t bits = mm[h];
-                        const uint32_t base = 64 * tid + 32 * h;
-                        while (bits) {
-                            const uint32_t b = __ffs(bits) - 1;
-                            bits &= bits - 1;
-                            sm.u.stage[r++] = (uint16_t)(base + b);
-                        }
-                    }
-                }
-                at += tot;
-            }
-            __syncthreads();  // (b) the slot is assembled
-            uint4 *dst = reinterpret_cast<uint4 *>(a.stage + (size_t)tile * a.stage_cap);
-            const uint4 *srcs = reinterpret_cast<const uint4 *>(sm.u.stage);
-            for (uint32_t o = tid; o < (start + 7) / 8; o += SS_THREADS) dst[o] = srcs[o];
-        }
-        __syncthreads();  // (c) shared memory is reused by the next tile
+    mine_any = __reduce_or_sync(0xFFFFFFFFu, mine_any);
+    if (lane == 0 && mine_any) atomicOr(&sm.active, mine_any);
+    __syncthreads();
+    const uint32_t active = sm.active;
+    if (active == 0) {
+        if (tid < NP) a.counts[(size_t)tid * a.ld + tile] = 0;
+        if (tid == 0) a.overflow[tile] = 0;
+        return;
     }
+    // counts, two patterns per word; inclusive warp scans of the words that
+    // hold a pattern with hits (tile totals stay below 2^16)
+    uint32_t packed[NQ], inc[NQ];
+#pragma unroll
+    for (uint32_t q = 0; q < NQ; q++) packed[q] = 0;
+#pragma unroll
+    for (uint32_t p = 0; p < NP; p++)
+        packed[p >> 1] |= (uint32_t)(__popc(m4[p].x) + __popc(m4[p].y)) << (16 * (p & 1));
+#pragma unroll
+    for (uint32_t q = 0; q < NQ; q++) {
+        inc[q] = packed[q];
+        if ((active >> (2 * q)) & 3u) {  // uniform
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc[q], o);
+                if ((int)lane >= o) inc[q] += t;
+            }
+        }
+        if (lane == 31) warp_sum[warp][q] = inc[q];
+    }
+    __syncthreads();
+    uint32_t before[NQ], total[NQ];
+#pragma unroll
+    for (uint32_t q = 0; q < NQ; q++) {
+        before[q] = total[q] = 0;
+        if ((active >> (2 * q)) & 3u)
+            for (uint32_t w = 0; w < SR_THREADS / 32; w++) {
+                const uint32_t x = warp_sum[w][q];
+                before[q] += w < warp ? x : 0u;
+                total[q] += x;
+            }
+    }
+    // tile totals per pattern, and where each pattern's hits start in the slot;
+    // the slot is assembled in shared memory (the staged text is no longer
+    // read) and stored with 16-byte writes
+    static_assert(kSearchStageCap * 2 <= kSearchTile, "the slot fits where the tile text was");
+    uint16_t *stage = reinterpret_cast<uint16_t *>(sm.text);
+    uint32_t start = 0;
+#pragma unroll
+    for (uint32_t p = 0; p < NP; p++) {
+        const uint32_t sh = 16 * (p & 1);
+        const uint32_t tot = (total[p >> 1] >> sh) & 0xFFFFu;
+        const uint32_t mine = (packed[p >> 1] >> sh) & 0xFFFFu;
+        uint32_t r = start + ((before[p >> 1] >> sh) & 0xFFFFu) + ((inc[p >> 1] >> sh) & 0xFFFFu) - mine;
+        if (mine && start + tot <= a.stage_cap) {
+            const uint32_t mm[2] = {m4[p].x, m4[p].y};
+#pragma unroll
+            for (uint32_t h = 0; h < 2; h++) {
+                uint32_t bits = mm[h];
+                while (bits) {
+                    const uint32_t b = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    stage[r++] = (uint16_t)((4 * tid + 2 * h + (b >> 4)) * 16 + (b & 15));
+                }
+            }
+        }
+        if (tid == 0) a.counts[(size_t)p * a.ld + tile] = tot;
+        start += tot;
+    }
+    if (tid == 0) {
+        a.overflow[tile] = start > a.stage_cap ? 1 : 0;
+        if (start > a.stage_cap) a.overflow_list[atomicAdd(a.overflow_n, 1u)] = tile;
+    }
+    if (start > a.stage_cap) return;  // uniform: recomputed later
+    __syncthreads();
+    uint4 *dst = reinterpret_cast<uint4 *>(a.stage + (size_t)tile * a.stage_cap);
+    const uint4 *src = reinterpret_cast<const uint4 *>(stage);
+    for (uint32_t o = tid; o < (start + 7) / 8; o += SR_THREADS) dst[o] = src[o];
 }
 
 // Pass 2 of the staged path: two warps per tile. Lane p reads pattern p's
@@ -841,27 +609,12 @@ void search_add_pattern(SearchArgs &a, const uint8_t *host, const uint8_t *dev, 
 
 constexpr uint32_t kSearchWriteGrid = 512;  // blocks of the staged form's write pass
 
-// Persistent grid of the stage pass: every block that fits on the device at
-// once (measured once per pattern count), at most one per tile.
-template <uint32_t NP>
-static uint32_t stage_grid(uint32_t n_tiles) {
-    static uint32_t resident = 0;  // per instantiation; a benign race computes the same value
-    if (resident == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_stage_kernel<NP>, SS_THREADS, 0);
-        resident = (uint32_t)std::max(1, sms * std::max(per_sm, 1));
-    }
-    return std::min(n_tiles, resident);
-}
-
 template <uint32_t NP>
 static cudaError_t launch_search_np(const SearchArgs &a, cudaStream_t st) {
     if (a.stage) {
         cudaError_t e0 = cudaMemsetAsync(a.overflow_n, 0, sizeof(uint32_t), st);
         if (e0 != cudaSuccess) return e0;
-        search_stage_kernel<NP><<<stage_grid<NP>(a.n_tiles), SS_THREADS, 0, st>>>(a); OL_LAUNCHED();
+        search_stage_kernel<NP><<<a.n_tiles, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();
         cudaError_t e = launch_scan_columns(a.counts, a.bases, a.totals, a.n_tiles, a.np, a.ld, st);
         if (e != cudaSuccess) return e;
         search_copy_kernel<<<(a.n_tiles + SC_TILES - 1) / SC_TILES, SR_THREADS, 0, st>>>(a); OL_LAUNCHED();

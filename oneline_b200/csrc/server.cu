@@ -3,8 +3,11 @@
 // crates/oneline-gpu/src/parser.rs). Requests are queued as they arrive and
 // taken by worker threads, each with its own context and CUDA stream.
 //
-// Continuous batching: a worker that frees up takes every request queued at
-// that moment (up to a step's limits) and serves them together:
+// Continuous batching: a worker that frees up takes its share of the requests
+// queued at that moment (the queue divided among the idle workers, up to a
+// step's limits) and serves them together; under light load a step is one
+// request and the workers serve requests side by side, under load the steps
+// grow:
 //   * admission first: each parse request reserves its estimated resident
 //     bytes against the store budget, counting the reservations of requests
 //     still in flight on other workers; least recently used idle documents
@@ -15,7 +18,10 @@
 //     then split into resident documents with one copy launch;
 //   * search requests on the same resident document are merged into one
 //     pattern set and one dictionary pass, and each request gets its own slice
-//     of the (pattern, offset)-ordered hits.
+//     of the (pattern, offset)-ordered hits;
+//   * a step serves its searches before its parses (a search never waits for
+//     a parse of its own step: it names a document that already exists), and
+//     each request's result is published as soon as it is ready.
 // Workers run steps concurrently, so requests that arrive while others are on
 // the GPU start on the next free worker and their kernels overlap on the
 // device. Results (offsets, kinds and the four tree arrays of a parse; counts
@@ -45,8 +51,8 @@ using namespace ol;
 
 namespace {
 
-constexpr uint32_t kStepMaxRequests = 256;             // requests one step takes at most
-constexpr uint64_t kStepMaxParseBytes = 256ull << 20;  // parse text one step takes at most
+constexpr uint32_t kStepMaxRequests = 256;            // requests one step takes at most
+constexpr uint64_t kStepMaxParseBytes = 64ull << 20;  // parse text one step takes at most
 constexpr uint64_t kStagingBytes = 64ull << 20;        // pinned download staging per worker (grown on demand)
 constexpr uint64_t kStagingMaxBytes = 2ull << 30;
 
@@ -154,6 +160,7 @@ struct ol_server {
     std::deque<Request *> queue;
     bool stopping = false;
     bool paused = false;  // workers take no request while set (ol_server_pause)
+    uint32_t idle = 0;    // workers waiting for requests
     std::mutex rmu;
     std::condition_variable rcv;
     std::unordered_map<uint64_t, ol_request_result> results;
@@ -489,6 +496,15 @@ void run_search_group(ol_server *s, ol_ctx *ctx, Staging &stg, uint64_t doc_id, 
     }
 }
 
+void publish(ol_server *s, const std::vector<ol_request_result *> &done) {
+    if (done.empty()) return;
+    {
+        std::lock_guard<std::mutex> g(s->rmu);
+        for (auto *x : done) s->results[x->id] = *x;
+    }
+    s->rcv.notify_all();
+}
+
 // One step: the requests taken from the queue together.
 void run_step(ol_server *s, uint32_t w, std::vector<Request *> &step) {
     ol_ctx *ctx = s->ctxs[w];
@@ -506,7 +522,7 @@ void run_step(ol_server *s, uint32_t w, std::vector<Request *> &step) {
     }
     // Admission of the parse requests, before any work.
     std::vector<Request *> parses;
-    std::vector<ol_request_result *> parse_res;
+    std::vector<ol_request_result *> parse_res, refused;
     std::vector<Entry> evicted;
     {
         std::lock_guard<std::mutex> g(s->smu);
@@ -518,6 +534,7 @@ void run_step(ol_server *s, uint32_t w, std::vector<Request *> &step) {
                 res[i].status = OL_ERR_ADMISSION;
                 res[i].end_ns = now_ns();
                 s->refusals++;
+                refused.push_back(&res[i]);
                 continue;
             }
             r->reserved = need;
@@ -527,9 +544,11 @@ void run_step(ol_server *s, uint32_t w, std::vector<Request *> &step) {
         }
     }
     free_entries(evicted);
-    if (!parses.empty()) run_parses(s, ctx, stg, parses, parse_res);
-    // Search requests, merged per document.
+    publish(s, refused);
+    // Search requests first (short, and never waiting on a parse of this
+    // step), merged per document; each group's results go out when done.
     std::map<uint64_t, std::vector<SearchPart>> groups;
+    std::vector<ol_request_result *> bad;
     for (size_t i = 0; i < step.size(); i++) {
         Request *r = step[i];
         if (r->kind != 1) continue;
@@ -537,17 +556,23 @@ void run_step(ol_server *s, uint32_t w, std::vector<Request *> &step) {
             res[i].status = OL_ERR_BAD_PATTERN;
             res[i].doc_id = r->doc_id;
             res[i].end_ns = now_ns();
+            bad.push_back(&res[i]);
             continue;
         }
         groups[r->doc_id].push_back(SearchPart{r, &res[i]});
     }
-    for (auto &kv : groups) run_search_group(s, ctx, stg, kv.first, kv.second);
-    for (Request *r : step) delete r;
-    {
-        std::lock_guard<std::mutex> g(s->rmu);
-        for (auto &x : res) s->results[x.id] = x;
+    publish(s, bad);
+    for (auto &kv : groups) {
+        run_search_group(s, ctx, stg, kv.first, kv.second);
+        std::vector<ol_request_result *> done;
+        for (auto &x : kv.second) done.push_back(x.res);
+        publish(s, done);
     }
-    s->rcv.notify_all();
+    if (!parses.empty()) {
+        run_parses(s, ctx, stg, parses, parse_res);
+        publish(s, parse_res);
+    }
+    for (Request *r : step) delete r;
     s->steps++;
     s->served += step.size();
     uint64_t big = s->largest_step.load();
@@ -562,10 +587,15 @@ void worker(ol_server *s, uint32_t w) {
         std::vector<Request *> step;
         {
             std::unique_lock<std::mutex> lk(s->qmu);
+            s->idle++;
             s->qcv.wait(lk, [&] { return s->stopping || (!s->paused && !s->queue.empty()); });
+            s->idle--;
             if (s->queue.empty()) break;
+            // this worker's share of the queue: the rest is left to the idle ones
+            const uint64_t share = (s->queue.size() + s->idle) / (s->idle + 1);
+            const uint64_t take = std::min<uint64_t>(limit, std::max<uint64_t>(share, 1));
             uint64_t parse_bytes = 0;
-            while (!s->queue.empty() && step.size() < limit) {
+            while (!s->queue.empty() && step.size() < take) {
                 Request *r = s->queue.front();
                 if (!step.empty() && r->kind == 0 && parse_bytes + r->len > kStepMaxParseBytes) break;
                 if (r->kind == 0) parse_bytes += r->len;
