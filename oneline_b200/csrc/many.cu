@@ -636,9 +636,6 @@ __global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArg
     }
     const uint32_t w0 = b * DH_WORDS + warp * (DH_WORDS / (DH_THREADS / 32));
     constexpr uint32_t kRounds = DH_WORDS / (DH_THREADS / 32) / 32;  // 16
-    // ManyHits (not the pair of arrays) into a 16-byte aligned array: pairs of
-    // hits per store
-    const bool pairs = !a.hit_off && ((uintptr_t)a.hits & 15) == 0;
     uint32_t c = 0;
     for (uint32_t r = 0; r < kRounds; r++) {
         const uint32_t idx = w0 + r * 32 + lane;
@@ -675,41 +672,16 @@ __global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArg
             }
         }
         __syncwarp();
-        if (pairs && cached) {
-            // ManyHits two per lane: the round's hits of id d go to slots
-            // [S, S + T), S = its base + rank; lane q of a pass takes the slot
-            // pair {2P, 2P + 1} (P from S / 2 on) and stores both with one
-            // 16-byte streaming store, or the one slot of a pair that the
-            // range cuts.
-            for (uint32_t d = 0; d < n_dup; d++) {
-                const unsigned long long S = dup_base[d] + rank;
-                const unsigned long long P0 = S >> 1, P1 = (S + T + 1) >> 1;  // pairs [P0, P1)
-                const uint32_t id = dup_id[d];
-                for (unsigned long long P = P0 + lane; P < P1; P += 32) {
-                    const unsigned long long s0 = 2 * P;
-                    const bool in0 = s0 >= S && s0 < S + T, in1 = s0 + 1 >= S && s0 + 1 < S + T;
-                    const bool fit1 = s0 + 1 < a.max_hits;
-                    if (in0 && in1 && fit1) {
-                        const uint32_t j0 = (uint32_t)(s0 - S);  // j0 + 1 < T
-                        __stcs(reinterpret_cast<uint4 *>(a.hits + s0), make_uint4(id, buf[j0], id, buf[j0 + 1]));
-                    } else {
-                        if (in0) put_hit(a, s0, id, buf[s0 - S]);
-                        if (in1) put_hit(a, s0 + 1, id, buf[s0 + 1 - S]);
-                    }
-                }
-            }
-        } else {
-            for (uint32_t base = 0; base < T; base += 32) {
-                const uint32_t j = base + lane;
-                if (j < T) {
-                    const uint32_t off = buf[j];
-                    if (cached) {
-                        for (uint32_t d = 0; d < n_dup; d++) put_hit(a, dup_base[d] + rank + j, dup_id[d], off);
-                    } else {
-                        for (uint32_t d = d0; d < d1; d++) {
-                            const uint32_t id = __ldg(a.dup_ids + d);
-                            put_hit(a, a.id_base[id] + rank + j, id, off);
-                        }
+        for (uint32_t base = 0; base < T; base += 32) {
+            const uint32_t j = base + lane;
+            if (j < T) {
+                const uint32_t off = buf[j];
+                if (cached) {
+                    for (uint32_t d = 0; d < n_dup; d++) put_hit(a, dup_base[d] + rank + j, dup_id[d], off);
+                } else {
+                    for (uint32_t d = d0; d < d1; d++) {
+                        const uint32_t id = __ldg(a.dup_ids + d);
+                        put_hit(a, a.id_base[id] + rank + j, id, off);
                     }
                 }
             }
