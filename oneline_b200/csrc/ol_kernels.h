@@ -139,6 +139,7 @@ struct SearchArgs {
     SearchPatMeta meta[kSearchMaxPatterns];
     uint32_t anchor_hash[kSearchMaxPatterns * 4];  // anchor-map bits of the patterns of >= 8 bytes
     uint32_t n_anchor;
+    uint32_t len_class[3];  // bit p: pattern p has <= 4 bytes; 5..7 bytes; 8 or more (search_add_pattern)
 };
 constexpr uint32_t kSearchStageCap = 8192;  // staged hits per tile (all patterns of a launch)
 

@@ -214,15 +214,8 @@ __device__ __forceinline__ void filter_tile(const SearchArgs &a, SearchSmem &sm,
             }
         }
     };
-    uint32_t shorts = 0, mids = 0, anchored = 0;  // patterns in `mask` by length: <= 4, 5-7, >= 8
-#pragma unroll
-    for (uint32_t p = 0; p < NP; p++) {
-        const uint32_t m = sm.pat[p].len;
-        if (!((mask >> p) & 1u)) continue;
-        if (m <= 4) shorts |= 1u << p;
-        else if (m < kAnchorMin) mids |= 1u << p;
-        else anchored |= 1u << p;
-    }
+    // patterns in `mask` by length: <= 4, 5-7, >= 8
+    const uint32_t shorts = a.len_class[0] & mask, mids = a.len_class[1] & mask, anchored = a.len_class[2] & mask;
     uint32_t cand = 0;  // bit 4p + k: piece k has a candidate of pattern p (patterns over 4 bytes)
 #pragma unroll
     for (uint32_t k = 0; k < SR_STEPS; k++) {
@@ -297,6 +290,7 @@ __device__ __forceinline__ void filter_tile(const SearchArgs &a, SearchSmem &sm,
             }
         }
     }
+    if (!__any_sync(0xFFFFFFFFu, cand != 0)) return;  // no candidate in the warp: nothing to verify
 #pragma unroll 1
     for (uint32_t bits = mids | anchored; bits; bits &= bits - 1) {
         const uint32_t p = __ffs(bits) - 1;
@@ -444,27 +438,26 @@ __global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) 
     for (uint32_t o = tid; o < NP * SR_PIECES / 8; o += SR_THREADS)
         reinterpret_cast<uint4 *>(&match[0][0])[o] = make_uint4(0, 0, 0, 0);
     __syncthreads();
-    filter_tile<NP>(a, sm, (1u << NP) - 1u, t0,
-                    [&](uint32_t p, uint32_t piece, uint32_t mk) { match[p][piece] = (uint16_t)mk; });
-    __syncthreads();
-    // my hits per pattern (4 pieces: at most 64), and the patterns with hits
-    // anywhere in the tile: a tile without hits is done here
-    uint2 m4[NP];
-    uint32_t mine_any = 0;
-#pragma unroll
-    for (uint32_t p = 0; p < NP; p++) {
-        m4[p] = *reinterpret_cast<const uint2 *>(&match[p][4 * tid]);
-        mine_any |= (m4[p].x | m4[p].y) ? 1u << p : 0u;
-    }
-    mine_any = __reduce_or_sync(0xFFFFFFFFu, mine_any);
-    if (lane == 0 && mine_any) atomicOr(&sm.active, mine_any);
+    // the patterns with hits anywhere in the tile, as the filter finds them
+    uint32_t found = 0;
+    filter_tile<NP>(a, sm, (1u << NP) - 1u, t0, [&](uint32_t p, uint32_t piece, uint32_t mk) {
+        match[p][piece] = (uint16_t)mk;
+        found |= (mk != 0 ? 1u : 0u) << p;
+    });
+    found = __reduce_or_sync(0xFFFFFFFFu, found);
+    if (lane == 0 && found) atomicOr(&sm.active, found);
     __syncthreads();
     const uint32_t active = sm.active;
-    if (active == 0) {
+    if (active == 0) {  // a tile without hits is done here
         if (tid < NP) a.counts[(size_t)tid * a.ld + tile] = 0;
         if (tid == 0) a.overflow[tile] = 0;
         return;
     }
+    // my hits per pattern with hits (4 pieces: at most 64)
+    uint2 m4[NP];
+#pragma unroll
+    for (uint32_t p = 0; p < NP; p++)
+        m4[p] = ((active >> p) & 1u) ? *reinterpret_cast<const uint2 *>(&match[p][4 * tid]) : make_uint2(0, 0);
     // counts, two patterns per word; inclusive warp scans of the words that
     // hold a pattern with hits (tile totals stay below 2^16)
     uint32_t packed[NQ], inc[NQ];
@@ -597,6 +590,7 @@ void search_add_pattern(SearchArgs &a, const uint8_t *host, const uint8_t *dev, 
     SearchPatMeta &m = a.meta[p];
     m = SearchPatMeta{};
     m.len = len;
+    a.len_class[len <= 4 ? 0 : len < kAnchorMin ? 1 : 2] |= 1u << p;
     m.f4 = (len ? host[0] : 0u) * 0x01010101u;
     for (uint32_t j = 0; j < 4 && j < len; j++) m.pre[j] = host[j] * 0x01010101u;
     if (len >= kAnchorMin)

@@ -468,10 +468,12 @@ void run_search_group(ol_server *s, ol_ctx *ctx, Staging &stg, uint64_t doc_id, 
     if (!found) {
         for (auto &x : parts) x.res->status = OL_ERR_NOT_FOUND;
     } else {
+        // The merged pass uses the staging the worker already holds and never
+        // grows it: pinned allocations are slow and freeing pinned memory waits
+        // for the whole device, which would stall every worker.
         uint64_t cap = 0;
         for (auto &x : parts) cap += hit_cap_of(s, x.r);
-        cap = std::min<uint64_t>(std::max<uint64_t>(cap, kStagingBytes / sizeof(ol_hit)),
-                                 kStagingMaxBytes / sizeof(ol_hit) - 8);
+        cap = std::min<uint64_t>(cap, (stg.bytes - 64) / sizeof(ol_hit));
         bool overflow = false;
         ol_status st = parts.size() > 1 ? search_pass(s, ctx, stg, e, parts, cap, overflow) : OL_OK;
         if (st == OL_OK && (overflow || parts.size() == 1)) {
