@@ -1100,6 +1100,24 @@ def serve_run(reqs, workers: int, warm_docs, coalesce: bool):
     return results, wall, stats
 
 
+def serve_timeline(ok, windows: int = 6) -> list:
+    """Latency over the stream: per window of submit time, the requests, their
+    p99 latency, the longest service (ms) and the kind and bytes of that request."""
+    t0 = min(r[6] for r in ok)
+    span = max(r[6] for r in ok) - t0 + 1
+    out = []
+    for w in range(windows):
+        sel = [r for r in ok if (r[6] - t0) * windows // span == w]
+        if not sel:
+            continue
+        lat = np.array([r[2] for r in sel], np.float64) / 1e6
+        slow = max(sel, key=lambda r: r[5] - r[4])
+        out.append({"from_s": round(w * span / windows / 1e9, 1), "requests": len(sel),
+                    "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                    "max_service_ms": round((slow[5] - slow[4]) / 1e6, 3), "slowest": [slow[0], int(slow[3])]})
+    return out
+
+
 def serve_record(args, local) -> dict:
     """The serving workload: the same open-loop stream against the served form
     (`serve_workers` workers, continuous batching) and the plain form (one
@@ -1131,7 +1149,8 @@ def serve_record(args, local) -> dict:
                      "service_p99_ms": round(float(np.percentile(svc, 99)), 3),
                      "p99_ms_by_kind": {k: round(float(np.percentile(v, 99)), 3) for k, v in by_kind.items() if v.size},
                      "req_per_s": round(len(ok) / wall, 1), "gb_per_s": round(nbytes / span / 1e9, 3),
-                     "wall_s": round(wall, 2), "store": stats, "clocks": clocks.summary()}
+                     "wall_s": round(wall, 2), "store": stats, "clocks": clocks.summary(),
+                     "timeline": serve_timeline(ok)}
     sv, pl = out["served"], out["plain"]
     # the same mix offered faster than one request per step can serve
     overload = {}

@@ -44,6 +44,18 @@ struct DocStats {
 
 // ---------------------------------------------------------- memory access --
 
+// Asks L2 to fetch [p, p + bytes) from device memory ahead of its use: one
+// bulk prefetch that returns no data and that nothing waits on. p 16-byte
+// aligned, bytes a multiple of 16, the range inside one allocation.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// How far ahead (in tiles) a one-tile-per-block kernel prefetches its text:
+// about the blocks resident at once over the GPU (148 SMs, 5-7 blocks each),
+// so the prefetched tile is one that a block starting soon reads.
+constexpr uint32_t kPrefetchTilesAhead = 1024;
+
 // Streaming 16-byte load (read once: do not keep in L1).
 __device__ __forceinline__ uint4 ld_stream16(const void *p) {
     uint4 v;

@@ -336,8 +336,12 @@ __global__ void __launch_bounds__(PT_THREADS, 6) parse_tiles_kernel(ParseArgs a)
 }
 
 // Staged form, pass 1: every tile counts its newlines and stages its lines.
+// Block b first asks L2 to prefetch the tile kPrefetchTilesAhead further on
+// (when this launch covers it), which a block that starts soon will read.
 __global__ void __launch_bounds__(PT_THREADS, 6) parse_stage_kernel(ParseArgs a) {
     __shared__ ParseSmem sm;
+    if (threadIdx.x == 0 && blockIdx.x + kPrefetchTilesAhead < gridDim.x)  // inside this launch's tiles
+        prefetch_l2(a.text + (uint64_t)(a.first_tile + blockIdx.x + kPrefetchTilesAhead) * kParseTile, kParseTile);
     parse_tile<true>(a, sm, a.first_tile + blockIdx.x);
 }
 

@@ -2,7 +2,9 @@
 //
 // Up to eight patterns are searched in one pass over the text; CTA b owns the
 // 16 KiB tile b and stages it, plus a halo of (longest pattern - 1) bytes, in
-// shared memory with 16-byte coalesced loads. Every 16-byte piece is compared
+// shared memory with 16-byte coalesced loads (in the stage pass, after asking
+// L2 to prefetch the tile kPrefetchTilesAhead further on, which a block that
+// starts soon will read). Every 16-byte piece is compared
 // with each pattern of up to 4 bytes at all sixteen starts at once (byte SWAR
 // on the piece shifted by 1, 2 and 3 bytes, built once for all patterns),
 // which decides it. Longer patterns only mark candidate pieces: 5-7 byte ones
@@ -433,6 +435,8 @@ __global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;
     const uint64_t t0 = (uint64_t)tile * kSearchTile;
+    if (tid == 0 && tile + kPrefetchTilesAhead < a.n_tiles)
+        prefetch_l2(a.text + (uint64_t)(tile + kPrefetchTilesAhead) * kSearchTile, kSearchTile);
     load_tile(a, sm, t0);
     if (tid == 0) sm.active = 0;
     for (uint32_t o = tid; o < NP * SR_PIECES / 8; o += SR_THREADS)
