@@ -457,6 +457,50 @@ __global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) 
         if (tid == 0) a.overflow[tile] = 0;
         return;
     }
+    uint16_t *stage = reinterpret_cast<uint16_t *>(sm.text);  // the slot, assembled where the text was
+    if ((active & (active - 1)) == 0) {  // hits of one pattern only: the usual tile
+        const uint32_t p = __ffs(active) - 1;
+        const uint2 m = *reinterpret_cast<const uint2 *>(&match[p][4 * tid]);
+        const uint32_t mine = __popc(m.x) + __popc(m.y);
+        uint32_t inc = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if ((int)lane >= o) inc += t;
+        }
+        if (lane == 31) warp_sum[warp][0] = inc;
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < SR_THREADS / 32; w++) {
+            const uint32_t x = warp_sum[w][0];
+            before += w < warp ? x : 0u;
+            total += x;
+        }
+        if (tid < NP) a.counts[(size_t)tid * a.ld + tile] = tid == p ? total : 0u;
+        const bool over = total > a.stage_cap;
+        if (tid == 0) {
+            a.overflow[tile] = over ? 1 : 0;
+            if (over) a.overflow_list[atomicAdd(a.overflow_n, 1u)] = tile;
+        }
+        if (over) return;  // uniform: recomputed later
+        uint32_t r = before + inc - mine;
+        const uint32_t mm[2] = {m.x, m.y};
+#pragma unroll
+        for (uint32_t h = 0; h < 2; h++) {
+            uint32_t bits = mm[h];
+            while (bits) {
+                const uint32_t b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                stage[r++] = (uint16_t)((4 * tid + 2 * h + (b >> 4)) * 16 + (b & 15));
+            }
+        }
+        __syncthreads();
+        uint4 *dst = reinterpret_cast<uint4 *>(a.stage + (size_t)tile * a.stage_cap);
+        const uint4 *src = reinterpret_cast<const uint4 *>(stage);
+        for (uint32_t o = tid; o < (total + 7) / 8; o += SR_THREADS) dst[o] = src[o];
+        return;
+    }
     // my hits per pattern with hits (4 pieces: at most 64)
     uint2 m4[NP];
 #pragma unroll
@@ -498,7 +542,6 @@ __global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) 
     // the slot is assembled in shared memory (the staged text is no longer
     // read) and stored with 16-byte writes
     static_assert(kSearchStageCap * 2 <= kSearchTile, "the slot fits where the tile text was");
-    uint16_t *stage = reinterpret_cast<uint16_t *>(sm.text);
     uint32_t start = 0;
 #pragma unroll
     for (uint32_t p = 0; p < NP; p++) {
@@ -535,7 +578,7 @@ __global__ void __launch_bounds__(SR_THREADS) search_stage_kernel(SearchArgs a) 
 // Pass 2 of the staged path: two warps per tile. Lane p reads pattern p's
 // count and first output slot (all patterns at once: one memory round trip),
 // a warp scan places each pattern's hits in the tile's slot, and the warps
-// copy them to their final slots, alternate runs of 128 each.
+// copy them to their final slots, alternate runs of 256 each.
 constexpr uint32_t SC_WARPS = 2;                          // warps per tile
 constexpr uint32_t SC_TILES = SR_THREADS / 32 / SC_WARPS;  // tiles per block
 __global__ void __launch_bounds__(SR_THREADS) search_copy_kernel(SearchArgs a) {
@@ -566,17 +609,17 @@ __global__ void __launch_bounds__(SR_THREADS) search_copy_kernel(SearchArgs a) {
         const uint32_t lim = b >= mx ? 0u : min(np_, mx - b);  // the first max_out hits overall
         uint32_t *__restrict__ out = a.out[p] + b;
         const uint16_t *__restrict__ src = slot + start;
-        // the tile's warps take alternate runs of 128 hits; four independent
+        // the tile's warps take alternate runs of 256 hits; eight independent
         // loads in flight per lane before the stores
-        for (uint32_t i0 = half * 128; i0 < lim; i0 += 128 * SC_WARPS) {
-            uint32_t v[4];
+        for (uint32_t i0 = half * 256; i0 < lim; i0 += 256 * SC_WARPS) {
+            uint32_t v[8];
 #pragma unroll
-            for (uint32_t j = 0; j < 4; j++) {
+            for (uint32_t j = 0; j < 8; j++) {
                 const uint32_t i = i0 + j * 32 + lane;
                 v[j] = i < lim ? __ldg(src + i) : 0u;
             }
 #pragma unroll
-            for (uint32_t j = 0; j < 4; j++) {
+            for (uint32_t j = 0; j < 8; j++) {
                 const uint32_t i = i0 + j * 32 + lane;
                 if (i < lim) out[i] = (uint32_t)(t0 + v[j]);
             }
