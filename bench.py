@@ -964,6 +964,26 @@ def batch_record(args, world, rank, local, p=None) -> dict:
     launches = L.ol_launch_count() - l0
     assert got == total
     dt = allreduce_max(dt, world)
+    # where one batched step's time goes: CUDA-event passes, and each call's
+    # host wall time
+    _, prof = p._profiled(batched)
+    passes = {}
+    for label, sec in prof.gpu_passes:
+        passes[label] = round(passes.get(label, 0.0) + sec * 1e3, 3)
+    calls = {}
+    h = ctypes.c_void_p()
+    t_0 = time.perf_counter()
+    chk(L.ol_batch_upload(p.ctx, data.data_ptr(), offs.ctypes.data, n_docs, ctypes.byref(h)))
+    t_1 = time.perf_counter()
+    chk(L.ol_batch_build_trees(p.ctx, h.value))
+    t_2 = time.perf_counter()
+    chk(L.ol_batch_search_many(p.ctx, h.value, ps.handle, total, 0, cnt.ctypes.data, ctypes.byref(tot), hits.data_ptr()))
+    t_3 = time.perf_counter()
+    L.ol_batch_free(h.value)
+    p.sync()
+    t_4 = time.perf_counter()
+    calls = {"ol_batch_upload": round((t_1 - t_0) * 1e3, 2), "ol_batch_build_trees": round((t_2 - t_1) * 1e3, 2),
+             "ol_batch_search_many": round((t_3 - t_2) * 1e3, 2), "ol_batch_free": round((t_4 - t_3) * 1e3, 2)}
     t0 = time.perf_counter()
     got_plain = plain()
     p.sync()
@@ -991,7 +1011,7 @@ def batch_record(args, world, rank, local, p=None) -> dict:
                         "timing": "host wall clock around the blocking batch calls (the value itself)",
                         "path": "ol_batch_upload (pinned) + ol_batch_build_trees + ol_batch_search_many (hits in HBM)"},
                 "gpu_launches": int(launches), "launches_per_step": round(launches / max(args.steps, 1), 1),
-                "clocks": clocks.summary(), "device": p.adapter_name()}
+                "passes_ms": passes, "calls_ms": calls, "clocks": clocks.summary(), "device": p.adapter_name()}
     return line
 
 

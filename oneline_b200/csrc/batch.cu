@@ -125,6 +125,38 @@ __global__ void batch_split_kernel(const BatchSplitDoc *__restrict__ docs, const
     if ((threadIdx.x & 31) == 0 && deepest) atomicMax(max_depth + lo, deepest);
 }
 
+// Item `blockIdx.x` of the documents' items (item_start: the prefix sum of
+// batch_pack_items): the document's bytes [64 KiB k, 64 KiB (k + 1)), and its
+// separator in its last item.
+__global__ void batch_pack_kernel(const BatchPackDoc *__restrict__ docs, const uint32_t *__restrict__ item_start,
+                                  uint32_t n, const uint8_t *__restrict__ in, uint8_t *__restrict__ text) {
+    const uint32_t item = blockIdx.x;
+    uint32_t lo = 0, hi = n;  // the last document i with item_start[i] <= item
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(item_start + mid) <= item)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    const BatchPackDoc d = docs[lo];
+    const uint64_t b0 = (uint64_t)(item - __ldg(item_start + lo)) * kBatchPackBytes;
+    const uint64_t b1 = min(d.len, b0 + kBatchPackBytes);
+    const uint8_t *src = in + d.src;
+    uint8_t *dst = text + d.dst;
+    for (uint64_t j = b0 + threadIdx.x; j < b1; j += blockDim.x) dst[j] = src[j];
+    if (d.sep && threadIdx.x == 0 && b0 + kBatchPackBytes >= d.len) dst[d.len] = '\n';
+}
+
+uint32_t batch_pack_items(uint64_t len) { return (uint32_t)std::max<uint64_t>((len + kBatchPackBytes - 1) / kBatchPackBytes, 1); }
+
+cudaError_t launch_batch_pack(const BatchPackDoc *docs, const uint32_t *item_start, uint32_t n, uint32_t items,
+                              const uint8_t *in, uint8_t *text, cudaStream_t st) {
+    if (n == 0 || items == 0) return cudaSuccess;
+    batch_pack_kernel<<<items, 256, 0, st>>>(docs, item_start, n, in, text); OL_LAUNCHED();
+    return cudaGetLastError();
+}
+
 uint32_t batch_split_items(uint64_t text_len, uint32_t lines) {
     const uint64_t a = (text_len + kSplitBytes - 1) / kSplitBytes, b = (lines + kSplitLines - 1) / kSplitLines;
     return (uint32_t)std::max<uint64_t>(std::max(a, b), 1);

@@ -303,6 +303,19 @@ cudaError_t launch_batch_tree_fixup(const uint32_t *line_start, uint32_t n, uint
                                     uint32_t *next_sibling, cudaStream_t st);
 cudaError_t launch_dict_emit(const DictEmitArgs &a, cudaStream_t st);
 
+// One document of a batch copied from the caller's bytes (uploaded as they
+// lie) to its place in the batch text: len bytes from in + src to text + dst,
+// then a '\n' at text + dst + len when sep is set (batch_pack).
+struct BatchPackDoc {
+    uint64_t src, dst, len;
+    uint32_t sep, pad;
+};
+// Work items of a document (batch_pack_kernel: kBatchPackBytes each, at least one).
+constexpr uint32_t kBatchPackBytes = 65536;
+uint32_t batch_pack_items(uint64_t len);
+cudaError_t launch_batch_pack(const BatchPackDoc *docs, const uint32_t *item_start, uint32_t n, uint32_t items,
+                              const uint8_t *in, uint8_t *text, cudaStream_t st);
+
 // One document of a batch and the buffers it is copied into (batch_split).
 struct BatchSplitDoc {
     uint64_t text_start, text_len;  // bytes of the batch text

@@ -187,12 +187,14 @@ __device__ __forceinline__ void parse_tile(const ParseArgs &a, ParseSmem &sm, ui
 
     // 2. Newline bits and their ranks within the warp: steps (0,1) and (2,3)
     //    packed in 16-bit fields.
-    uint32_t z[PT_STEPS][4];
+    uint32_t nlm[PT_STEPS];  // bit b: byte b of the thread's piece in step k is a newline
     uint32_t cnt[PT_STEPS];
 #pragma unroll
     for (uint32_t k = 0; k < PT_STEPS; k++) {
-        newline_bits(v[k], k * 4096 + tid * 16, valid, z[k]);
-        cnt[k] = __popc(z[k][0]) + __popc(z[k][1]) + __popc(z[k][2]) + __popc(z[k][3]);
+        uint32_t z[4];
+        newline_bits(v[k], k * 4096 + tid * 16, valid, z);
+        nlm[k] = gather16(z[0], z[1], z[2], z[3]);
+        cnt[k] = __popc(nlm[k]);
     }
     uint32_t c01 = cnt[0] | (cnt[1] << 16), c23 = cnt[2] | (cnt[3] << 16);
     uint32_t i01 = c01, i23 = c23;
@@ -272,7 +274,7 @@ __device__ __forceinline__ void parse_tile(const ParseArgs &a, ParseSmem &sm, ui
             if (rk > (int32_t)PT_LIST) continue;
             // one loop over the piece's 16-bit newline mask: the warp runs as
             // many rounds as its busiest lane has newlines in this piece
-            uint32_t m = gather16(z[k][0], z[k][1], z[k][2], z[k][3]);
+            uint32_t m = nlm[k];
             while (m) {
                 const uint32_t b = __ffs(m) - 1;
                 m &= m - 1;

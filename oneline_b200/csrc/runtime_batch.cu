@@ -29,15 +29,11 @@ struct ol_batch {
     uint32_t *d_line_start = nullptr;
 };
 
-// The batch of documents parts[i][0 .. lens[i]) (host memory), uploaded and
-// parsed (see ol_batch_upload).
-ol_status ol::batch_from_parts(ol_ctx *ctx, const uint8_t *const *parts, const uint64_t *lens, uint32_t n,
-                               ol_batch **out) {
-    *out = nullptr;
-    // Layout: document bytes, then '\n' when the document is non-empty and does
-    // not already end in one.
-    auto b = new ol_batch();
-    b->ctx = ctx;
+namespace {
+
+// Lays n documents end to end, each non-empty one that does not end in '\n'
+// followed by one: their starts and lengths go to b; returns the text length.
+uint64_t batch_layout(ol_batch *b, const uint8_t *const *parts, const uint64_t *lens, uint32_t n) {
     b->n = n;
     b->start.resize(n);
     b->len.resize(n);
@@ -48,16 +44,18 @@ ol_status ol::batch_from_parts(ol_ctx *ctx, const uint8_t *const *parts, const u
         b->len[i] = l;
         T += l + ((l && parts[i][l - 1] != '\n') ? 1 : 0);
     }
-    if (T > OL_MAX_GPU_INPUT_LEN) {
-        delete b;
-        return ctx_fail(ctx, OL_ERR_INPUT_TOO_LARGE, "batch text of " + std::to_string(T) + " bytes exceeds the 32-bit limit");
-    }
-    std::lock_guard<std::recursive_mutex> g(ctx->mu);
-    cudaSetDevice(ctx->device);
+    return T;
+}
+
+bool needs_separator(const ol_batch *b, uint32_t i) {
+    const uint64_t next = i + 1 < b->n ? b->start[i + 1] : b->doc->text_len;
+    return next > b->start[i] + b->len[i];
+}
+
+// Fills the batch text through the pinned ring (any host memory): documents
+// and separators packed on the host, 16 MiB per copy.
+cudaError_t batch_fill_ring(ol_ctx *ctx, ol_batch *b, const uint8_t *const *parts) {
     cudaStream_t st = ctx->stream;
-    ol_status s = new_doc(ctx, T, &b->doc);
-    cudaError_t e = cudaSuccess;
-    // Pack through the pinned ring: documents and separators, 16 MiB per copy.
     uint64_t at = 0, ring_i = 0, fill = 0;
     uint8_t *slot = nullptr;
     auto flush = [&]() -> cudaError_t {
@@ -92,12 +90,90 @@ ol_status ol::batch_from_parts(ol_ctx *ctx, const uint8_t *const *parts, const u
         return cudaSuccess;
     };
     static const uint8_t nl = '\n';
-    for (uint32_t i = 0; s == OL_OK && e == cudaSuccess && i < n; i++) {
-        const uint64_t l = b->len[i];
-        if (l) e = put(parts[i], l);
-        if (e == cudaSuccess && l && parts[i][l - 1] != '\n') e = put(&nl, 1);
+    cudaError_t e = cudaSuccess;
+    for (uint32_t i = 0; e == cudaSuccess && i < b->n; i++) {
+        if (b->len[i]) e = put(parts[i], b->len[i]);
+        if (e == cudaSuccess && needs_separator(b, i)) e = put(&nl, 1);
     }
-    if (s == OL_OK && e == cudaSuccess) e = flush();
+    if (e == cudaSuccess) e = flush();
+    return e;
+}
+
+// Fills the batch text from page-locked host memory: the documents' bytes
+// [in_off[0], in_off[n]) of data cross PCIe in one copy as they lie, then
+// batch_pack_kernel moves every document to its place and writes its
+// separator, so the host copies nothing.
+cudaError_t batch_fill_pinned(ol_ctx *ctx, ol_batch *b, const uint8_t *data, const uint64_t *in_off) {
+    cudaStream_t st = ctx->stream;
+    const uint32_t n = b->n;
+    const uint64_t in_bytes = in_off[n] - in_off[0];
+    std::vector<BatchPackDoc> docs(n);
+    std::vector<uint32_t> item_start(n + 1);
+    uint64_t items = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        docs[i] = BatchPackDoc{in_off[i] - in_off[0], b->start[i], b->len[i], needs_separator(b, i) ? 1u : 0u, 0u};
+        item_start[i] = (uint32_t)items;
+        items += batch_pack_items(b->len[i]);
+    }
+    item_start[n] = (uint32_t)items;
+    if (items > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+    const size_t table = ((size_t)n * sizeof(BatchPackDoc) + (size_t)(n + 1) * 4 + 255) & ~(size_t)255;
+    DevBuf tmp;
+    cudaError_t e = tmp.reserve(table + std::max<uint64_t>(in_bytes, 16), st);
+    uint8_t *base = (uint8_t *)tmp.ptr;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base, docs.data(), (size_t)n * sizeof(BatchPackDoc), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(base + (size_t)n * sizeof(BatchPackDoc), item_start.data(), (size_t)(n + 1) * 4,
+                            cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && in_bytes) {
+        GpuPass pass(ctx, "batch upload: copy to device");
+        e = cudaMemcpyAsync(base + table, data + in_off[0], in_bytes, cudaMemcpyHostToDevice, st);
+    }
+    if (e == cudaSuccess) {
+        GpuPass pass(ctx, "batch upload: lay out documents");
+        e = launch_batch_pack((const BatchPackDoc *)base, (const uint32_t *)(base + (size_t)n * sizeof(BatchPackDoc)), n,
+                              (uint32_t)items, base + table, b->doc->text, st);
+    }
+    tmp.release(st);  // stream-ordered: freed after the pack
+    // the pageable tables must stay until their copies are done
+    cudaError_t s2 = cudaStreamSynchronize(st);
+    return e != cudaSuccess ? e : s2;
+}
+
+bool is_page_locked(const void *p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+// Uploads the laid-out documents (from parts, or when `pinned` is set from
+// page-locked data at in_off), parses the text and builds the document tables.
+ol_status batch_build(ol_ctx *ctx, const uint8_t *const *parts, const uint64_t *lens, uint32_t n, const uint8_t *pinned,
+                      const uint64_t *in_off, ol_batch **out) {
+    *out = nullptr;
+    auto b = new ol_batch();
+    b->ctx = ctx;
+    const uint64_t T = batch_layout(b, parts, lens, n);
+    if (T > OL_MAX_GPU_INPUT_LEN) {
+        delete b;
+        return ctx_fail(ctx, OL_ERR_INPUT_TOO_LARGE, "batch text of " + std::to_string(T) + " bytes exceeds the 32-bit limit");
+    }
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    ol_status s = new_doc(ctx, T, &b->doc);
+    cudaError_t e = cudaSuccess;
+    if (s == OL_OK) {
+        if (pinned) {
+            e = batch_fill_pinned(ctx, b, pinned, in_off);
+        } else {
+            GpuPass pass(ctx, "batch upload: pack on the host and copy");
+            e = batch_fill_ring(ctx, b, parts);
+        }
+    }
     if (s == OL_OK && e != cudaSuccess) s = ctx_cuda(ctx, e, "batch upload");
     if (s == OL_OK && T) s = parse_doc(ctx, b->doc, T / 24 + 4096, nullptr);
     // Document ranges and first lines on the device.
@@ -129,6 +205,15 @@ ol_status ol::batch_from_parts(ol_ctx *ctx, const uint8_t *const *parts, const u
     return OL_OK;
 }
 
+}  // namespace
+
+// The batch of documents parts[i][0 .. lens[i]) (host memory), uploaded and
+// parsed (see ol_batch_upload).
+ol_status ol::batch_from_parts(ol_ctx *ctx, const uint8_t *const *parts, const uint64_t *lens, uint32_t n,
+                               ol_batch **out) {
+    return batch_build(ctx, parts, lens, n, nullptr, nullptr, out);
+}
+
 extern "C" ol_status ol_batch_upload(ol_ctx *ctx, const uint8_t *data, const uint64_t *doc_offsets, uint32_t n,
                                      ol_batch **out) {
     if (!ctx || !out || !doc_offsets || n == 0) return OL_ERR_INVALID_ARG;
@@ -142,7 +227,10 @@ extern "C" ol_status ol_batch_upload(ol_ctx *ctx, const uint8_t *data, const uin
         parts[i] = data ? data + doc_offsets[i] : nullptr;
         lens[i] = doc_offsets[i + 1] - doc_offsets[i];
     }
-    return batch_from_parts(ctx, parts.data(), lens.data(), n, out);
+    // page-locked input crosses PCIe as it lies and is laid out on the device
+    const bool pinned = doc_offsets[n] > doc_offsets[0] && is_page_locked(data + doc_offsets[0]) &&
+                        is_page_locked(data + doc_offsets[n] - 1);
+    return batch_build(ctx, parts.data(), lens.data(), n, pinned ? data : nullptr, doc_offsets, out);
 }
 
 extern "C" void ol_batch_free(ol_batch *b) {
@@ -184,8 +272,13 @@ extern "C" ol_status ol_batch_build_trees(ol_ctx *ctx, ol_batch *b) {
     const uint32_t L = b->doc->line_count;
     uint32_t *p = (uint32_t *)t->parent_buf.ptr, *e = (uint32_t *)t->end_buf.ptr, *fc = (uint32_t *)t->fc_buf.ptr,
              *ns = (uint32_t *)t->ns_buf.ptr;
-    cudaError_t ce = launch_batch_tree_fixup(b->d_line_start, b->n, L, b->doc->kinds, p, e, fc, p, e, fc, ns, ctx->stream);
+    cudaError_t ce;
+    {
+        GpuPass pass(ctx, "batch: links kept inside documents");
+        ce = launch_batch_tree_fixup(b->d_line_start, b->n, L, b->doc->kinds, p, e, fc, p, e, fc, ns, ctx->stream);
+    }
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+    prof_mark(ctx, "batch: wait for the links");
     return ctx_cuda(ctx, ce, "batch trees");
 }
 

@@ -84,3 +84,43 @@ def test_dictionary_hits_per_document(parser, heavy_min_hits):
         sel = doc_of == i
         assert np.array_equal(hits["pattern"][sel], hp), i
         assert np.array_equal(hits["offset"][sel] - np.uint32(starts[i]), ho), i
+
+
+def test_same_batch_from_page_locked_buffer(parser):
+    """Page-locked input crosses PCIe as it lies and the device lays the
+    documents out (separators included): per document the same lines, kinds,
+    links and dictionary hits, also when the documents start inside the buffer."""
+    import torch
+
+    docs = make_docs(6, 120)
+    data = np.frombuffer(b"".join(docs), np.uint8)
+    pad = 37
+    h = torch.empty(data.size + pad + 5, dtype=torch.uint8, pin_memory=True)
+    hv = h.numpy()
+    hv[:] = ord("|")
+    hv[pad: pad + data.size] = data
+    offs = np.zeros(len(docs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(d) for d in docs])
+    offs += np.uint64(pad)
+    b = parser.upload_batch((hv, offs))
+    ref = parser.upload_batch(docs)  # pageable: packed on the host
+    assert b.text_len() == ref.text_len()
+    parser.build_batch_trees(b)
+    for i, d in enumerate(docs):
+        offs_i, nodes = oracle.parse(d)
+        got = parser.read_batch_doc(b, i)
+        assert np.array_equal(got["offsets"], offs_i), i
+        assert np.array_equal(got["kinds"], nodes["kind"].astype(np.uint8)), i
+        want = oracle.full_tree(nodes)
+        for k in ("parent", "subtree_end", "first_child", "next_sibling"):
+            assert np.array_equal(got[k], want[k]), (i, k)
+    pats = datagen.patterns_dictionary(data, 6, n=200) + [b"\n|||", b"|| \n"]
+    ps = parser.compile_patterns(None, pats, max_patterns=None)
+    outs = []
+    for x in (b, ref):
+        counts, total = parser.batch_search_many(x, ps, 0, 0)
+        buf = torch.full((2 * max(total, 1),), -1, dtype=torch.int32, device="cuda")
+        counts, t = parser.batch_search_many(x, ps, buf.data_ptr(), total)
+        assert t == total
+        outs.append((counts, buf.cpu().numpy()[: 2 * total]))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
