@@ -955,10 +955,13 @@ def batch_record(args, world, rank, local, p=None) -> dict:
     p.sync()
     barrier(world)
     l0 = L.ol_launch_count()
+    step_ms = []
     with ClockSampler(local) as clocks:
         t0 = time.perf_counter()
         for _ in range(args.steps):
+            ts = time.perf_counter()
             got = batched()
+            step_ms.append((time.perf_counter() - ts) * 1e3)
         p.sync()
         dt = (time.perf_counter() - t0) / args.steps
     launches = L.ol_launch_count() - l0
@@ -970,6 +973,7 @@ def batch_record(args, world, rank, local, p=None) -> dict:
     passes = {}
     for label, sec in prof.gpu_passes:
         passes[label] = round(passes.get(label, 0.0) + sec * 1e3, 3)
+    host_steps = [(label, round(sec * 1e3, 3)) for label, sec in prof.host_steps]
     calls = {}
     h = ctypes.c_void_p()
     t_0 = time.perf_counter()
@@ -1011,7 +1015,10 @@ def batch_record(args, world, rank, local, p=None) -> dict:
                         "timing": "host wall clock around the blocking batch calls (the value itself)",
                         "path": "ol_batch_upload (pinned) + ol_batch_build_trees + ol_batch_search_many (hits in HBM)"},
                 "gpu_launches": int(launches), "launches_per_step": round(launches / max(args.steps, 1), 1),
-                "passes_ms": passes, "calls_ms": calls, "clocks": clocks.summary(), "device": p.adapter_name()}
+                "step_ms": {"min": round(min(step_ms), 2), "median": round(statistics.median(step_ms), 2),
+                            "max": round(max(step_ms), 2)},
+                "passes_ms": passes, "host_steps_ms": host_steps, "calls_ms": calls, "clocks": clocks.summary(),
+                "device": p.adapter_name()}
     return line
 
 

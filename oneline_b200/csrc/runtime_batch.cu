@@ -175,7 +175,9 @@ ol_status batch_build(ol_ctx *ctx, const uint8_t *const *parts, const uint64_t *
         }
     }
     if (s == OL_OK && e != cudaSuccess) s = ctx_cuda(ctx, e, "batch upload");
+    prof_mark(ctx, "batch upload: documents in device memory");
     if (s == OL_OK && T) s = parse_doc(ctx, b->doc, T / 24 + 4096, nullptr);
+    prof_mark(ctx, "batch upload: parse");
     // Document ranges and first lines on the device.
     const size_t tbytes = (size_t)n * 16 + (size_t)(n + 1) * 4;
     if (s == OL_OK) {
@@ -196,6 +198,7 @@ ol_status batch_build(ol_ctx *ctx, const uint8_t *const *parts, const uint64_t *
             e = cudaMemcpyAsync(b->line_start.data(), b->d_line_start, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) s = ctx_cuda(ctx, e, "batch tables");
+        prof_mark(ctx, "batch upload: document tables");
     }
     if (s != OL_OK) {
         ol_batch_free(b);
