@@ -40,6 +40,7 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -167,7 +168,9 @@ struct ol_server {
     std::atomic<uint64_t> next_id{1}, next_doc{1};
     std::mutex smu;
     std::unordered_map<uint64_t, Entry> store;
+    std::set<std::pair<uint64_t, uint64_t>> lru;  // (last_use, document id) of every resident document
     uint64_t used = 0, reserved = 0, tick = 0;
+    uint64_t busy = 0;  // bytes of the resident documents in use (refs > 0)
     std::atomic<uint64_t> evictions{0}, refusals{0}, steps{0}, served{0}, largest_step{0};
 };
 
@@ -193,24 +196,27 @@ uint64_t estimate_resident(const uint8_t *text, uint64_t len) {
 // Called with smu held; returns false, evicting nothing, when the documents in
 // use and the reservations leave no room.
 bool make_room(ol_server *s, uint64_t need, std::vector<Entry> &evicted) {
-    uint64_t busy = s->reserved;
-    for (auto &kv : s->store)
-        if (kv.second.refs) busy += kv.second.bytes;
-    if (busy + need > s->budget) return false;
+    if (s->reserved + s->busy + need > s->budget) return false;
+    // the least recently used first; documents in use are skipped (few)
+    auto it = s->lru.begin();
     while (s->used + s->reserved + need > s->budget) {
-        uint64_t victim = 0, best = UINT64_MAX;
-        for (auto &kv : s->store)
-            if (kv.second.refs == 0 && kv.second.last_use < best) {
-                best = kv.second.last_use;
-                victim = kv.first;
-            }
-        if (!victim) return false;
-        evicted.push_back(s->store[victim]);
+        while (it != s->lru.end() && s->store[it->second].refs) ++it;
+        if (it == s->lru.end()) return false;
+        auto victim = s->store.find(it->second);
+        evicted.push_back(victim->second);
         s->store.erase(victim);
+        it = s->lru.erase(it);
         s->used -= evicted.back().bytes;
         s->evictions++;
     }
     return true;
+}
+
+// Marks a resident document used now (the most recently used).
+void touch(ol_server *s, uint64_t id, Entry &e) {
+    s->lru.erase({e.last_use, id});
+    e.last_use = s->tick++;
+    s->lru.insert({e.last_use, id});
 }
 
 void free_entries(std::vector<Entry> &v) {
@@ -264,6 +270,7 @@ void commit_doc(ol_server *s, Request *r, ol_doc *&d, ol_tree *&t, ol_request_re
             e.last_use = s->tick++;
             res.doc_id = s->next_doc++;
             s->store[res.doc_id] = e;
+            s->lru.insert({e.last_use, res.doc_id});
             s->used += bytes;
             d = nullptr;
             t = nullptr;
@@ -459,8 +466,8 @@ void run_search_group(ol_server *s, ol_ctx *ctx, Staging &stg, uint64_t doc_id, 
         std::lock_guard<std::mutex> g(s->smu);
         auto it = s->store.find(doc_id);
         if (it != s->store.end()) {
-            it->second.refs++;
-            it->second.last_use = s->tick++;
+            if (it->second.refs++ == 0) s->busy += it->second.bytes;
+            touch(s, doc_id, it->second);
             e = it->second;
             found = true;
         }
@@ -489,7 +496,7 @@ void run_search_group(ol_server *s, ol_ctx *ctx, Staging &stg, uint64_t doc_id, 
         }
         std::lock_guard<std::mutex> g(s->smu);
         auto it = s->store.find(doc_id);
-        if (it != s->store.end()) it->second.refs--;
+        if (it != s->store.end() && --it->second.refs == 0) s->busy -= it->second.bytes;
     }
     prof_mark(ctx, "server: search step");
     for (auto &x : parts) {
@@ -690,6 +697,7 @@ extern "C" void ol_server_destroy(ol_server *s) {
         ol_doc_free(kv.second.doc);
     }
     s->store.clear();
+    s->lru.clear();
     for (ol_ctx *c : s->ctxs) ol_ctx_destroy(c);
     for (auto &g : s->staging)
         if (g.ptr) cudaFreeHost(g.ptr);

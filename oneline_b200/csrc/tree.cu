@@ -88,7 +88,7 @@ struct TreeSmem {
     __device__ uint32_t &a(uint32_t k, uint32_t t) { return fa[k * TR_THREADS + t]; }
     __device__ uint32_t &b(uint32_t k, uint32_t t) { return fb[k * TR_THREADS + t]; }
 };
-extern __shared__ uint32_t tree_dyn_smem[];
+extern __shared__ __align__(16) uint32_t tree_dyn_smem[];
 
 __device__ __forceinline__ TreeSmem tree_smem(uint32_t D) {
     TreeSmem s;
@@ -208,30 +208,55 @@ __global__ void __launch_bounds__(TR_THREADS, 5) tree_resolve_kernel(TreeArgs a)
     // Per level: exclusive max over the threads before mine (seeded with the
     // tiles before this one) and exclusive min over the threads after mine
     // (seeded with the tiles after this one).
+    // One warp per level; lane L holds the entries of threads 8L .. 8L+7 (two
+    // 16-byte loads), reduces them, and one warp scan of the 32 lane values
+    // gives each lane its seed.
     for (uint32_t k = warp; k < D; k += 8) {
-        uint32_t run = a.in_last[(size_t)tile * kTreeLevels + k];
-        for (uint32_t j = 0; j < TR_THREADS / 32; j++) {
-            uint32_t x = sm.a(k, j * 32 + lane), inc = x;
+        uint4 *ra = reinterpret_cast<uint4 *>(&sm.a(k, 8 * lane));
+        uint4 *rb = reinterpret_cast<uint4 *>(&sm.b(k, 8 * lane));
+        {
+            const uint4 q0 = ra[0], q1 = ra[1];
+            uint32_t v[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+            uint32_t inc = 0;
+#pragma unroll
+            for (int i = 0; i < 8; i++) inc = max(inc, v[i]);
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+                const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
                 if ((int)lane >= o) inc = max(inc, t);
             }
-            uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
-            sm.a(k, j * 32 + lane) = max(run, lane == 0 ? 0u : prev);
-            run = max(run, __shfl_sync(0xFFFFFFFFu, inc, 31));
+            const uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
+            uint32_t run = max(a.in_last[(size_t)tile * kTreeLevels + k], lane == 0 ? 0u : prev);
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const uint32_t t = v[i];
+                v[i] = run;
+                run = max(run, t);
+            }
+            ra[0] = make_uint4(v[0], v[1], v[2], v[3]);
+            ra[1] = make_uint4(v[4], v[5], v[6], v[7]);
         }
-        run = a.in_first[(size_t)tile * kTreeLevels + k];
-        for (int j = TR_THREADS / 32 - 1; j >= 0; j--) {
-            uint32_t x = sm.b(k, j * 32 + lane), inc = x;
+        {
+            const uint4 q0 = rb[0], q1 = rb[1];
+            uint32_t v[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+            uint32_t inc = NONE;
+#pragma unroll
+            for (int i = 0; i < 8; i++) inc = min(inc, v[i]);
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                uint32_t t = __shfl_down_sync(0xFFFFFFFFu, inc, o);
+                const uint32_t t = __shfl_down_sync(0xFFFFFFFFu, inc, o);
                 if (lane + o < 32) inc = min(inc, t);
             }
-            uint32_t next = __shfl_down_sync(0xFFFFFFFFu, inc, 1);
-            sm.b(k, j * 32 + lane) = min(run, lane == 31 ? NONE : next);
-            run = min(run, __shfl_sync(0xFFFFFFFFu, inc, 0));
+            const uint32_t next = __shfl_down_sync(0xFFFFFFFFu, inc, 1);
+            uint32_t run = min(a.in_first[(size_t)tile * kTreeLevels + k], lane == 31 ? NONE : next);
+#pragma unroll
+            for (int i = 7; i >= 0; i--) {
+                const uint32_t t = v[i];
+                v[i] = run;
+                run = min(run, t);
+            }
+            rb[0] = make_uint4(v[0], v[1], v[2], v[3]);
+            rb[1] = make_uint4(v[4], v[5], v[6], v[7]);
         }
     }
     __syncthreads();
