@@ -71,18 +71,28 @@ class GpuServer:
         self._keep = {}  # request id -> buffers that must outlive the request
         self._out = {}   # request id -> result arrays
 
-    def submit_parse(self, text, *, results: bool = False, cap: int | None = None) -> int:
+    def submit_parse(self, text, *, results: bool = False, cap: int | None = None, out: dict | None = None) -> int:
         """Queues a parse. With ``results``, the document's offsets, kinds and four
         tree arrays come back with the result (``cap`` lines of room; default: one
-        line per byte, always enough)."""
+        line per byte, always enough). ``out`` (implies ``results``): arrays to
+        write them into instead of new ones, as ``results`` returns them (u32
+        offsets and links, u8 kinds, all of one length, the room), so a client can
+        reuse its buffers; they must not be touched until the request is waited on."""
         buf = np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray)) else np.ascontiguousarray(text, np.uint8)
         rid = ctypes.c_uint64()
-        dest, out = None, None
-        if results:
+        dest = None
+        if out is not None:
+            n = int(out["offsets"].size)
+            for k, dt in (("offsets", np.uint32), ("kinds", np.uint8)) + tuple((k, np.uint32) for k in LINK_NAMES):
+                a = out[k]
+                if a.dtype != dt or a.size < n or not a.flags.c_contiguous:
+                    raise ValueError(f"out[{k!r}] must be a contiguous {np.dtype(dt).name} array of at least {n} entries")
+        elif results:
             n = int(cap if cap is not None else buf.size + 1)
             out = {"offsets": np.zeros(max(n, 1), np.uint32), "kinds": np.zeros(max(n, 1), np.uint8)}
             for k in LINK_NAMES:
                 out[k] = np.zeros(max(n, 1), np.uint32)
+        if out is not None:
             dest = ParseDest(n, *[out[k].ctypes.data for k in ("offsets", "kinds") + LINK_NAMES])
         st = _lib.load().ol_server_submit_parse_to(self._h, buf.ctypes.data, buf.size,
                                                    ctypes.byref(dest) if dest is not None else None,
@@ -94,16 +104,27 @@ class GpuServer:
             self._out[rid.value] = out
         return rid.value
 
-    def submit_search(self, doc_id: int, patterns, *, results: bool = False, max_hits: int | None = None) -> int:
+    def submit_search(self, doc_id: int, patterns, *, results: bool = False, max_hits: int | None = None,
+                      out: dict | None = None) -> int:
         """Queues a search of a resident document. With ``results``, the counts
-        and the first ``max_hits`` hits (pattern = index in ``patterns``) come back."""
+        and the first ``max_hits`` hits (pattern = index in ``patterns``) come back.
+        ``out`` (implies ``results``): {"counts": u32 array with room for every
+        pattern, "hits": HIT_DTYPE array} to write them into, for a client that
+        reuses its buffers (the hits array's size is the room)."""
         pats = [bytes(p) for p in patterns]
         bufs = [np.frombuffer(p, np.uint8) for p in pats]
         P = (ctypes.c_void_p * len(pats))(*[b.ctypes.data for b in bufs])
         lens = np.array([len(p) for p in pats], np.uint32)
         rid = ctypes.c_uint64()
-        dest, out = None, None
-        if results:
+        dest = None
+        if out is not None:
+            out = dict(out)
+            if (out["counts"].dtype != np.uint32 or out["counts"].size < len(pats) or out["hits"].dtype != HIT_DTYPE
+                    or not out["counts"].flags.c_contiguous or not out["hits"].flags.c_contiguous):
+                raise ValueError("out needs a contiguous u32 'counts' array with room for every pattern and a "
+                                 "contiguous HIT_DTYPE 'hits' array")
+            dest = SearchDest(int(out["hits"].size), out["counts"].ctypes.data, out["hits"].ctypes.data)
+        elif results:
             mh = int(max_hits if max_hits is not None else self.max_hits)
             out = {"counts": np.zeros(max(len(pats), 1), np.uint32), "hits": np.zeros(max(mh, 1), HIT_DTYPE)}
             dest = SearchDest(mh, out["counts"].ctypes.data, out["hits"].ctypes.data)

@@ -155,3 +155,40 @@ def test_admission_is_decided_before_any_work_and_counts_requests_in_flight():
         # alone, b fits (a, idle, is evicted)
         res_b2 = s.wait(s.submit_parse(b))
         assert res_b2.status == 0 and s.stats()["evictions"] == 1
+
+
+def test_results_into_reused_caller_buffers():
+    """A client that keeps its result buffers: each request writes into the
+    arrays it is given (`out=`), and a set reused for the next request holds
+    that request's result, equal to the oracle's."""
+    from oneline_b200 import HIT_DTYPE
+    from oneline_b200.serving import LINK_NAMES
+
+    texts, searches = workload()
+    room = max(t.count(b"\n") + 2 for t in texts)
+    pset = {"offsets": np.full(room, 7, np.uint32), "kinds": np.full(room, 7, np.uint8),
+            **{k: np.full(room, 7, np.uint32) for k in LINK_NAMES}}
+    sset = {"counts": np.zeros(64, np.uint32), "hits": np.zeros(1 << 16, HIT_DTYPE)}
+    with GpuServer(workers=2, store_budget=1 << 30) as s:
+        for t in texts:  # one set, reused request after request
+            rid = s.submit_parse(t, out=pset)
+            res = s.wait(rid)
+            a = s.results(rid, res)
+            offs, nodes = oracle.parse(t)
+            tr = oracle.full_tree(nodes)
+            assert res.status == 0
+            assert np.array_equal(a["offsets"], offs) and np.array_equal(a["kinds"], nodes["kind"].astype(np.uint8))
+            for k in LINK_NAMES:
+                assert np.array_equal(a[k], tr[k]), k
+            assert np.shares_memory(a["offsets"], pset["offsets"])
+            doc = res.doc_id
+            for pats in [p for i, p in searches if texts[i] is t]:
+                rid = s.submit_search(doc, pats, out=sset)
+                r = s.wait(rid)
+                h = s.results(rid, r)
+                counts, hp, ho = oracle.find_many(t, pats)
+                assert r.status == 0 and np.array_equal(h["counts"], counts.astype(np.uint32))
+                k = min(hp.size, sset["hits"].size)
+                assert np.array_equal(h["hits"]["pattern"], hp[:k]) and np.array_equal(h["hits"]["offset"], ho[:k])
+        with pytest.raises(ValueError):
+            s.submit_search(doc, [b"abcd"] * 65, out=sset)  # counts has room for 64 patterns
