@@ -651,9 +651,13 @@ __global__ void __launch_bounds__(DH_THREADS) dict_emit_heavy_kernel(DictEmitArg
     uint32_t rank = a.heavy_bases[(size_t)h * a.ld + b];
     for (uint32_t w = 0; w < warp; w++) rank += warp_tot[w];
     if (c == 0) return;  // uniform over the warp
+    // each round's bitmap word is loaded a round ahead, so its latency hides
+    // behind the previous round's listing and stores
+    uint32_t nxt = w0 + lane < a.n_words ? __ldg(col + w0 + lane) : 0u;
     for (uint32_t r = 0; r < kRounds; r++) {
         const uint32_t idx = w0 + r * 32 + lane;
-        const uint32_t word = idx < a.n_words ? __ldg(col + idx) : 0u;
+        const uint32_t word = nxt;
+        if (r + 1 < kRounds) nxt = idx + 32 < a.n_words ? __ldg(col + idx + 32) : 0u;
         const uint32_t cnt = __popc(word);
         uint32_t inc = cnt;
 #pragma unroll
