@@ -480,15 +480,16 @@ __global__ void __launch_bounds__(DS_THREADS) dict_sort_scatter_kernel(const uns
     for (uint32_t d = lane; d < 256; d += 32) cursor[warp][d] = start[d] + base[(size_t)d * ld + c];
     __syncwarp();
     const uint32_t lt = (1u << lane) - 1u;
+    unsigned long long nkey = c * kDictSortChunk + lane < n ? in[c * kDictSortChunk + lane] : 0ull;  // a step ahead
     for (uint32_t i = 0; i < DS_PER_LANE; i++) {
         const uint32_t idx = c * kDictSortChunk + i * 32 + lane;
         const bool valid = idx < n;
         const uint32_t vm = __ballot_sync(0xFFFFFFFFu, valid);
         if (!vm) break;
-        unsigned long long key = 0;
+        const unsigned long long key = nkey;
+        if (i + 1 < DS_PER_LANE) nkey = idx + 32 < n ? in[idx + 32] : 0ull;
         uint32_t d = 0, peers = 0;
         if (valid) {
-            key = in[idx];
             d = (uint32_t)(key >> shift) & 255u;
             peers = __match_any_sync(vm, d);
             out[cursor[warp][d] + __popc(peers & lt)] = key;
