@@ -143,10 +143,29 @@ __global__ void __launch_bounds__(1024) tree_scan_kernel(TreeArgs a) {
     const uint32_t T = a.n_tiles;
     const uint32_t per = (T + 1023) / 1024;
     const uint32_t lo = min(T, tid * per), hi = min(T, lo + per);
+    // Up to kHeld tiles per thread (2^23 lines) are read once, all loads in
+    // flight together, and kept in registers for the walks below.
+    constexpr uint32_t kHeld = 8;
+    const bool held = per <= kHeld;  // uniform
+    uint32_t vl[kHeld], vf[kHeld];
     uint32_t mx = 0, mn = NONE;
-    for (uint32_t t = lo; t < hi; t++) {
-        mx = max(mx, a.tile_last[(size_t)t * kTreeLevels + k]);
-        mn = min(mn, a.tile_first[(size_t)t * kTreeLevels + k]);
+    if (held) {
+#pragma unroll
+        for (uint32_t i = 0; i < kHeld; i++) {
+            const bool in = lo + i < hi;
+            vl[i] = in ? a.tile_last[(size_t)(lo + i) * kTreeLevels + k] : 0u;
+            vf[i] = in ? a.tile_first[(size_t)(lo + i) * kTreeLevels + k] : NONE;
+        }
+#pragma unroll
+        for (uint32_t i = 0; i < kHeld; i++) {
+            mx = max(mx, vl[i]);
+            mn = min(mn, vf[i]);
+        }
+    } else {
+        for (uint32_t t = lo; t < hi; t++) {
+            mx = max(mx, a.tile_last[(size_t)t * kTreeLevels + k]);
+            mn = min(mn, a.tile_first[(size_t)t * kTreeLevels + k]);
+        }
     }
     // inclusive scans over threads: max forward, min backward
     uint32_t imx = mx, imn = mn;
@@ -169,6 +188,21 @@ __global__ void __launch_bounds__(1024) tree_scan_kernel(TreeArgs a) {
     uint32_t ex_mx = max(before, lane == 0 ? 0u : up);
     uint32_t ex_mn = min(after, lane == 31 ? NONE : down);
     // walk my tiles: forward exclusive max, then backward exclusive min
+    if (held) {
+        uint32_t run = ex_mx;
+#pragma unroll
+        for (uint32_t i = 0; i < kHeld; i++) {
+            if (lo + i < hi) a.in_last[(size_t)(lo + i) * kTreeLevels + k] = run;
+            run = max(run, vl[i]);
+        }
+        run = ex_mn;
+#pragma unroll
+        for (int i = kHeld - 1; i >= 0; i--) {
+            if (lo + i < hi) a.in_first[(size_t)(lo + i) * kTreeLevels + k] = run;
+            run = min(run, vf[i]);
+        }
+        return;
+    }
     uint32_t run = ex_mx;
     for (uint32_t t = lo; t < hi; t++) {
         a.in_last[(size_t)t * kTreeLevels + k] = run;
