@@ -1,6 +1,9 @@
 // The parse-then-search pipeline of a resident document as one CUDA graph:
 // re-parse (newline count, column scan, tile parse, fix-up), tree links and a
-// multi-pattern search, captured once and replayed with a single launch. No
+// multi-pattern search, captured once and replayed with a single launch. The
+// graph has two branches: the parse and the tree on one private context's
+// stream, the search (which reads only the text) on a second one, so the
+// search's blocks fill the SMs that the parse's small passes leave idle. No
 // reference counterpart (the reference records wgpu command buffers per call,
 // crates/oneline-gpu/src/parser.rs).
 //
@@ -21,6 +24,8 @@ using namespace ol;
 
 struct ol_pipeline {
     ol_ctx *pctx = nullptr;  // private: its scratch is baked into the graph
+    ol_ctx *sctx = nullptr;  // private, the search branch's: its own stream and scratch
+    cudaEvent_t fork = nullptr, join = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     DevBuf patterns;
@@ -29,13 +34,20 @@ struct ol_pipeline {
 
 namespace {
 
-cudaError_t enqueue_step(ol_ctx *pctx, ol_doc *d, ol_tree *t, const uint8_t *const *hp,
+// The search reads only the text, which the parse does not write: it runs on
+// the second context's stream beside the parse and the tree.
+cudaError_t enqueue_step(ol_pipeline *p, ol_doc *d, ol_tree *t, const uint8_t *const *hp,
                          const std::vector<const uint8_t *> &dp, const std::vector<uint32_t> &lens,
                          const uint32_t *max_matches, uint32_t *d_totals, uint32_t *const *d_outs) {
-    cudaError_t e = enqueue_parse(pctx, d);
+    ol_ctx *pctx = p->pctx, *sctx = p->sctx;
+    cudaError_t e = cudaEventRecord(p->fork, pctx->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(sctx->stream, p->fork, 0);
+    if (e == cudaSuccess) e = enqueue_parse(pctx, d);
     if (e == cudaSuccess) e = enqueue_tree(pctx, d, t);
     if (e == cudaSuccess && !dp.empty())
-        e = launch_multi(pctx, d, hp, dp.data(), lens.data(), (uint32_t)dp.size(), max_matches, d_totals, d_outs);
+        e = launch_multi(sctx, d, hp, dp.data(), lens.data(), (uint32_t)dp.size(), max_matches, d_totals, d_outs);
+    if (e == cudaSuccess) e = cudaEventRecord(p->join, sctx->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(pctx->stream, p->join, 0);
     return e;
 }
 
@@ -48,7 +60,11 @@ extern "C" void ol_pipeline_free(ol_pipeline *p) {
     if (p->pctx) {
         cudaSetDevice(p->pctx->device);
         cudaStreamSynchronize(p->pctx->stream);
+        if (p->sctx) cudaStreamSynchronize(p->sctx->stream);
         p->patterns.release(p->pctx->stream);
+        if (p->fork) cudaEventDestroy(p->fork);
+        if (p->join) cudaEventDestroy(p->join);
+        if (p->sctx) ol_ctx_destroy(p->sctx);
         ol_ctx_destroy(p->pctx);
     }
     delete p;
@@ -81,6 +97,15 @@ extern "C" ol_status ol_pipeline_capture(ol_ctx *ctx, ol_doc *d, ol_tree *t, con
     }
     ol_ctx *pc = p->pctx;
     pc->tune = ctx->tune;
+    s = ol_ctx_create(ctx->device, &p->sctx);
+    if (s == OL_OK && (cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess ||
+                       cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming) != cudaSuccess))
+        s = OL_ERR_CUDA;
+    if (s != OL_OK) {
+        ol_pipeline_free(p);
+        return ctx_fail(ctx, s, "pipeline: could not create its search context");
+    }
+    p->sctx->tune = ctx->tune;
     // pattern copies, 16-byte aligned
     std::vector<size_t> at(n);
     size_t w = 0;
@@ -97,19 +122,20 @@ extern "C" ol_status ol_pipeline_capture(ol_ctx *ctx, ol_doc *d, ol_tree *t, con
     for (uint32_t i = 0; i < n; i++) dp[i] = (const uint8_t *)p->patterns.ptr + at[i];
     // One plain run sizes every scratch buffer; the capture must then allocate nothing.
     const uint64_t l0 = ol_launch_count();
-    if (e == cudaSuccess) e = enqueue_step(pc, d, t, patterns, dp, ln, max_matches, d_totals, d_outs);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(pc->stream);  // the pattern copies
+    if (e == cudaSuccess) e = enqueue_step(p, d, t, patterns, dp, ln, max_matches, d_totals, d_outs);
     if (e == cudaSuccess) e = cudaStreamSynchronize(pc->stream);
     p->kernels = (uint32_t)(ol_launch_count() - l0);
-    void *before[8] = {pc->scratch_a.ptr, pc->scratch_b.ptr,   pc->scratch_c.ptr, t->parent_buf.ptr, t->end_buf.ptr,
-                       p->patterns.ptr,   pc->parse_slot.ptr, pc->search_stage.ptr};
+    void *before[8] = {pc->scratch_a.ptr, pc->scratch_b.ptr,   p->sctx->scratch_a.ptr, t->parent_buf.ptr, t->end_buf.ptr,
+                       p->patterns.ptr,   pc->parse_slot.ptr, p->sctx->search_stage.ptr};
     if (e == cudaSuccess) e = cudaStreamBeginCapture(pc->stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        cudaError_t ce = enqueue_step(pc, d, t, patterns, dp, ln, max_matches, d_totals, d_outs);
+        cudaError_t ce = enqueue_step(p, d, t, patterns, dp, ln, max_matches, d_totals, d_outs);
         e = cudaStreamEndCapture(pc->stream, &p->graph);
         if (ce != cudaSuccess) e = ce;
     }
-    void *after[8] = {pc->scratch_a.ptr, pc->scratch_b.ptr,   pc->scratch_c.ptr, t->parent_buf.ptr, t->end_buf.ptr,
-                      p->patterns.ptr,   pc->parse_slot.ptr, pc->search_stage.ptr};
+    void *after[8] = {pc->scratch_a.ptr, pc->scratch_b.ptr,   p->sctx->scratch_a.ptr, t->parent_buf.ptr, t->end_buf.ptr,
+                      p->patterns.ptr,   pc->parse_slot.ptr, p->sctx->search_stage.ptr};
     if (e == cudaSuccess && memcmp(before, after, sizeof before) != 0) e = cudaErrorStreamCaptureInvalidated;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
     if (e != cudaSuccess) {
