@@ -233,8 +233,10 @@ ol_status ol_query(ol_ctx *ctx, const uint8_t *text, uint64_t len, const uint32_
  *      tree links (into `tree`, already built for it) and a search of n
  *      patterns (as ol_search_multi_async: d_totals, d_outs on the device);
  *      ol_pipeline_launch then replays all of it with one graph launch on the
- *      pipeline's own stream. The pipeline keeps private scratch memory; the
- *      document, tree and output buffers must outlive it. */
+ *      pipeline's own stream; inside the graph the search runs on a second
+ *      branch beside the parse and the tree. The pipeline keeps the scratch
+ *      memory of two private contexts; the document, tree and output buffers
+ *      must outlive it. */
 typedef struct ol_pipeline ol_pipeline;
 ol_status ol_pipeline_capture(ol_ctx *ctx, ol_doc *doc, ol_tree *tree, const uint8_t *const *patterns,
                               const uint32_t *lens, uint32_t n, const uint32_t *max_matches, uint32_t *d_totals,
