@@ -200,9 +200,17 @@ bool make_room(ol_server *s, uint64_t need, std::vector<Entry> &evicted) {
     // the least recently used first; documents in use are skipped (few)
     auto it = s->lru.begin();
     while (s->used + s->reserved + need > s->budget) {
-        while (it != s->lru.end() && s->store[it->second].refs) ++it;
+        auto victim = s->store.end();
+        while (it != s->lru.end()) {  // the index holds exactly the resident documents
+            victim = s->store.find(it->second);
+            if (victim == s->store.end()) {
+                it = s->lru.erase(it);
+                continue;
+            }
+            if (victim->second.refs == 0) break;
+            ++it;
+        }
         if (it == s->lru.end()) return false;
-        auto victim = s->store.find(it->second);
         evicted.push_back(victim->second);
         s->store.erase(victim);
         it = s->lru.erase(it);
