@@ -143,8 +143,9 @@ __global__ void __launch_bounds__(1024) tree_scan_kernel(TreeArgs a) {
     const uint32_t T = a.n_tiles;
     const uint32_t per = (T + 1023) / 1024;
     const uint32_t lo = min(T, tid * per), hi = min(T, lo + per);
-    // Up to kHeld tiles per thread (2^23 lines) are read once, all loads in
-    // flight together, and kept in registers for the walks below.
+    // Up to kHeld tiles per thread (documents of up to 2^25 lines) are read
+    // once, all loads in flight together, and kept in registers for the walks
+    // below.
     constexpr uint32_t kHeld = 8;
     const bool held = per <= kHeld;  // uniform
     uint32_t vl[kHeld], vf[kHeld];

@@ -68,3 +68,25 @@ def test_device_hit_digest_equals_the_cpu_ports_digest():
     assert bench.device_hit_digest(t, total, chunk=1000) == dg
     hits[2:4], hits[4:6] = hits[4:6].copy(), hits[2:4].copy()
     assert bench.device_hit_digest(torch.from_numpy(hits.view(np.int32).copy()), total) != dg
+
+
+def test_serve_client_buffers_have_room_and_are_reused():
+    """The serve client's result buffers: every parse gets a set with room for
+    its lines (the serve corpus has fewer than one line per 8 bytes), sets are
+    pooled per room, and search sets hold SERVE_MAX_HITS hits."""
+    import numpy as np
+
+    from oneline_b200 import HIT_DTYPE
+
+    for n in (0, 1, 1000, 64 << 10, (64 << 20) - 1, 64 << 20):
+        room = bench.serve_room(n)
+        assert room >= n // 8 + 4096 and room & (room - 1) == 0 and room >= 1 << 12
+    reqs = [("parse", 0.0, np.zeros(n, np.uint8)) for n in (1000, 1000, 5 << 20)]
+    reqs += [("search", 0.1, [b"abcd"], 0)]
+    pool = bench.serve_buffer_pool(reqs)
+    assert len(pool["search"]) == 128 and pool["search"][0]["hits"].dtype == HIT_DTYPE
+    assert pool["search"][0]["hits"].size == bench.SERVE_MAX_HITS
+    small, big = bench.serve_room(1000), bench.serve_room(5 << 20)
+    assert len(pool[small]) == 2 and len(pool[big]) == 1
+    s = pool[big][0]
+    assert all(a.size == big for a in s.values()) and s["kinds"].dtype == np.uint8 and s["offsets"].dtype == np.uint32
