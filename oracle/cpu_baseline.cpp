@@ -200,28 +200,42 @@ std::vector<std::pair<size_t, size_t>> partition(const uint8_t *b, size_t len, s
     return out;
 }
 
-// ANSV (links.rs:27-131): for each i the nearest j < i with keys[j] < keys[i]
-// (or <= when or_equal), NONE if there is none.
+// ANSV (links.rs:27-131): for each line the nearest line before it in scan
+// order (j < i when FORWARD, j > i otherwise) whose key is smaller (or, with
+// OR_EQUAL, smaller or equal); NONE if there is none. A line's key is its
+// depth, NONE for a blank line. Three phases, as the reference: each block of
+// BLOCK lines runs a stack (key and position together, so the keys are read
+// once, in order, from the nodes), the blocks' remaining stacks are chained in
+// scan order, and each block resolves its pending lines against the chain.
 constexpr size_t BLOCK = 1 << 15;
 constexpr uint32_t PENDING = NONE - 1;
 
-void nearest_previous(const uint32_t *keys, size_t n, bool or_equal, uint32_t *res, int threads) {
+inline uint32_t node_key(const Node &nd) { return nd.kind == 0 ? NONE : std::min(nd.depth, NONE - 1); }
+
+template <bool OR_EQUAL, bool FORWARD>
+void nearest_before(const Node *nodes, size_t n, uint32_t *res, int threads) {
     if (n == 0) return;
-    auto ok = [or_equal](uint32_t v, uint32_t x) { return or_equal ? v <= x : v < x; };
+    auto ok = [](uint32_t v, uint32_t x) { return OR_EQUAL ? v <= x : v < x; };
+    auto at = [n](size_t v) { return FORWARD ? v : n - 1 - v; };  // scan step -> line
+    struct KeyAt {
+        uint32_t key, idx;
+    };
     size_t nb = (n + BLOCK - 1) / BLOCK;
-    std::vector<std::vector<uint32_t>> summaries(nb);
+    std::vector<std::vector<KeyAt>> summaries(nb);
     parallel_for(threads, nb, [&](size_t b) {
         size_t base = b * BLOCK, end = std::min(n, base + BLOCK);
-        std::vector<uint32_t> stack;
-        for (size_t j = base; j < end; j++) {
-            uint32_t x = keys[j];
-            while (!stack.empty() && !ok(keys[stack.back()], x)) stack.pop_back();
-            res[j] = stack.empty() ? PENDING : stack.back();
-            stack.push_back((uint32_t)j);
+        std::vector<KeyAt> stack;
+        stack.reserve(256);
+        for (size_t v = base; v < end; v++) {
+            const size_t j = at(v);
+            const uint32_t x = node_key(nodes[j]);
+            while (!stack.empty() && !ok(stack.back().key, x)) stack.pop_back();
+            res[j] = stack.empty() ? PENDING : stack.back().idx;
+            stack.push_back(KeyAt{x, (uint32_t)j});
         }
         auto &s = summaries[b];
         for (size_t i = 0; i < stack.size(); i++) {
-            bool next_same = i + 1 < stack.size() && keys[stack[i + 1]] == keys[stack[i]];
+            bool next_same = i + 1 < stack.size() && stack[i + 1].key == stack[i].key;
             if (!next_same) s.push_back(stack[i]);
         }
     });
@@ -235,10 +249,10 @@ void nearest_previous(const uint32_t *keys, size_t n, bool or_equal, uint32_t *r
         heads[b] = head;
         auto &s = summaries[b];
         if (!s.empty()) {
-            uint32_t min_key = keys[s[0]];
+            uint32_t min_key = s[0].key;
             while (head != NONE && !ok(pool[head].key, min_key)) head = pool[head].link;
-            for (uint32_t v : s) {
-                pool.push_back(Entry{keys[v], v, head});
+            for (const KeyAt &e : s) {
+                pool.push_back(Entry{e.key, e.idx, head});
                 head = (uint32_t)(pool.size() - 1);
             }
         }
@@ -246,9 +260,10 @@ void nearest_previous(const uint32_t *keys, size_t n, bool or_equal, uint32_t *r
     parallel_for(threads, nb, [&](size_t b) {
         size_t base = b * BLOCK, end = std::min(n, base + BLOCK);
         uint32_t p = heads[b];
-        for (size_t j = base; j < end; j++) {
+        for (size_t v = base; v < end; v++) {
+            const size_t j = at(v);
             if (res[j] != PENDING) continue;
-            uint32_t x = keys[j];
+            const uint32_t x = node_key(nodes[j]);
             while (p != NONE && !ok(pool[p].key, x)) p = pool[p].link;
             res[j] = p == NONE ? NONE : pool[p].idx;
         }
@@ -351,28 +366,21 @@ uint64_t olb_parse_par(const uint8_t *text, uint64_t len, uint32_t *offsets, Nod
     return total;
 }
 
-// build_links (links.rs:135-180): parent + subtree_end.
+// build_links (links.rs:135-180): parent + subtree_end. The nearest smaller
+// line before each line is its parent; the nearest smaller-or-equal line after
+// it ends its subtree (the document's end when there is none).
 void olb_build_links(const Node *nodes, uint64_t n, uint32_t *parent, uint32_t *subtree_end, int threads) {
-    std::vector<uint32_t> keys(n), rev(n), rev_next(n);
+    nearest_before<false, true>(nodes, n, parent, threads);
+    nearest_before<true, false>(nodes, n, subtree_end, threads);
     size_t step = std::max<size_t>(1, (n + threads - 1) / std::max(threads, 1));
     size_t parts = (n + step - 1) / step;
     parallel_for(threads, parts, [&](size_t p) {
         for (size_t i = p * step; i < std::min<size_t>(n, (p + 1) * step); i++) {
-            uint32_t k = nodes[i].kind == 0 ? NONE : std::min(nodes[i].depth, NONE - 1);
-            keys[i] = k;
-            rev[n - 1 - i] = k;
-        }
-    });
-    nearest_previous(keys.data(), n, false, parent, threads);
-    nearest_previous(rev.data(), n, true, rev_next.data(), threads);
-    parallel_for(threads, parts, [&](size_t p) {
-        for (size_t i = p * step; i < std::min<size_t>(n, (p + 1) * step); i++) {
-            if (keys[i] == NONE) {
+            if (nodes[i].kind == 0) {
                 parent[i] = NONE;
                 subtree_end[i] = (uint32_t)i + 1;
-            } else {
-                uint32_t r = rev_next[n - 1 - i];
-                subtree_end[i] = r == NONE ? (uint32_t)n : (uint32_t)(n - 1 - r);
+            } else if (subtree_end[i] == NONE) {
+                subtree_end[i] = (uint32_t)n;
             }
         }
     });
